@@ -1,0 +1,365 @@
+"""Throughput of the PM step on B200: particle-steps/s at 512^3 particles /
+512^3 mesh, FP32 (and the same run in FP64 on the GPU), against the
+reference's own CPU code on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--mbits 9] [--f 1] [--no-fp64]
+
+A step is one leapfrog step of the solver (drift, CIC deposit, Poisson solve,
+gather + kick) over all particles. The workload is the 3D throughput box:
+N = 2^mbits particles per side on an (f N)^3 mesh, L = 500 Mpc/h, scale-free
+P(k) ~ k^-1.5 (sigma 0.83 at 8 Mpc/h, seeded Philox white noise), Zel'dovich
+start at a = 0.05 and da = 0.0475 (20 steps reach a = 1). Particle state
+(3.2 GB at 512^3 in FP32) and meshes are far larger than L2, so no L2 flush is
+needed between steps.
+
+Multi-GPU: the PM step does not shard (one box per GPU); N > 1 runs N
+independent replicas (seed + rank) with no data-path collective, timed as the
+max over ranks ("scaling": "weak").
+
+Output: one JSON line on rank 0 (see the keys below).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L_BOX, NS, A0, DA = 500.0, -1.5, 0.05, 0.0475
+METRIC = "PM particle-steps/s at 512^3 (FP32 vs FP64 GPU at P(k) err<1e-3); adjoint/fwd time"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mbits", type=int, default=9)
+    ap.add_argument("--f", type=int, default=1)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(mbits, f):
+    n = 1 << mbits
+    return f"pm3d_{n}^3_particles_{f * n}^3_mesh_L{int(L_BOX)}_ns{NS}"
+
+
+# ------------------------------------------------------------------ clocks --
+class Clocks:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ distributed --
+def dist_init(n):
+    if n <= 1:
+        return 0, 1, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ.get("RANK", 0))
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, dist.get_world_size(), dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(x, dist):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------- reference --
+def cpu_reference(mbits_sample=7, max_seconds=20.0, threads=None, max_steps=None):
+    """Times the reference's own Gravity<3>::drift+kick (oracle/_ref, compiled
+    from the reference sources; falls back to the CPU restatement) on a
+    bounded sample: a 128^3-particle / 128^3-mesh box with the throughput
+    box's cell size (L scaled to 125 Mpc/h), same spectrum and time step."""
+    import ctypes
+    import numpy as np
+    from oracle import cpu as oracle
+    n = 1 << mbits_sample
+    L = L_BOX * n / 512
+    noise = oracle.noise_mt19937(3, n ** 3)
+    phi = oracle.potential(3, mbits_sample, L, oracle.grf_scale_free(3, mbits_sample, L, NS, False, 8.0, 0.83, noise))
+    reflib = ROOT / "oracle" / "_ref" / "libconan_ref.so"
+    cores = threads or os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    steps = 0
+    total = 0.0
+    if reflib.exists():
+        R = ctypes.CDLL(str(reflib))
+        R.ref_time_steps.restype = ctypes.c_double
+        R.ref_max_threads.restype = ctypes.c_int
+        cores = R.ref_max_threads()
+        kind = "reference"
+        while total < max_seconds and (max_steps is None or steps < max_steps):
+            t_init = ctypes.c_double()
+            dt = R.ref_time_steps(3, n, 1, ctypes.c_double(L), ctypes.c_double(68.5), ctypes.c_double(1.0),
+                                  ctypes.c_double(0.0), phi.ctypes.data_as(ctypes.c_void_p), ctypes.c_double(A0),
+                                  ctypes.c_double(DA), 1, ctypes.byref(t_init))
+            total += dt
+            steps += 1
+    else:
+        kind = "port"
+        cores = 1
+        X, P = oracle.zeldovich(3, n, L, phi, A0, A0 + DA / 2)
+        a = A0
+        while total < max_seconds and (max_steps is None or steps < max_steps):
+            t0 = time.perf_counter()
+            oracle.drift(3, n, 68.5, 1.0, 0.0, X, P, a, DA)
+            oracle.kick(3, n, 1, L, 68.5, 1.0, 0.0, X, P, a + DA / 2, DA)
+            total += time.perf_counter() - t0
+            a += DA
+            steps += 1
+    value = n ** 3 * steps / total
+    return {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{steps} leapfrog step(s) of a {n}^3-particle/{n}^3-mesh box, L={L:g} Mpc/h "
+                      f"(cell size of the 512^3 box), ns={NS}, from a={A0}; reference FP64 CPU code, "
+                      f"{cores} OpenMP threads", "seconds": total, "steps": steps}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        pass  # the reference has no JIT or caches to warm; warm-up steps are not timed
+    r = cpu_reference(max_seconds=1e9, max_steps=max(1, args.steps))
+    line = {"metric": METRIC, "value": r["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": r["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded mt19937 white noise, scale-free GRF)", "impl": "reference",
+            "config": {"workload": workload_name(args.mbits, args.f), "sample": r["sample"]},
+            "cpu_baseline": {"value": r["value"], "unit": r["unit"], "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------- ours --
+def algorithmic_bytes(kernel, Np, Nc, fp64):
+    """Bytes a kernel must move by definition (FP32; x2 for FP64):
+    deposit 12 Np + 4 Nc (positions in, density out); gather+kick+drift
+    48 Np + 4 Nc (positions and momenta in and out, potential in)."""
+    s = 2 if fp64 else 1
+    if kernel.startswith("gather_kick"):
+        return s * (48 * Np + 4 * Nc)
+    if kernel == "deposit":
+        return s * (12 * Np + 4 * Nc)
+    return None
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import conan_b200 as cb
+
+    rank, world, dist = dist_init(args.gpus)
+    dev = int(os.environ.get("LOCAL_RANK", 0)) if args.gpus > 1 else 0
+    torch.cuda.set_device(dev)
+    mbits, f = args.mbits, args.f
+    n = 1 << mbits
+    Np, Nc = n ** 3, (f * n) ** 3
+    H = {"dim": 3, "mbits": mbits, "size": L_BOX, "ns": NS, "smooth": 0, "scale-free": 1, "scale": 8.0,
+         "sigma": 0.83, "seed": 3 + rank}
+    dens = cb.generate_random_field(H, precision="fp64", device=dev)
+    phi = cb.compute_potential(H, dens, precision="fp64", device=dev)
+    del dens
+    peaks = {}
+    try:
+        peaks = json.load(open(ROOT / "MEASURED_PEAKS.json"))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    def timed_run(prec, profile=False):
+        g = cb.Gravity(3, n, f, L_BOX, precision=prec, device=dev)
+        s = torch.cuda.ExternalStream(g.stream_ptr())
+        # warm-up: W steps from the initial conditions (plans, graphs, caches)
+        g.run(phi, A0, DA, args.warmup)
+        g.sync()
+        g.init(phi, A0, A0 + DA / 2)
+        g.set_profiling(profile)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier(dist)
+        torch.cuda.synchronize()
+        with Clocks(dev) as clk:
+            e0.record(s)
+            g.run(None, A0, DA, args.steps)
+            e1.record(s)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        barrier(dist)
+        prof = g.profile() if profile else {}
+        return g, ms, clk.summary(), prof
+
+    # FP32 product path (graph-captured run)
+    g32, ms32, clocks, _ = timed_run("fp32")
+    ms32 = max_over_ranks(ms32, dist)
+    k32, P32, cnt = g32.power_spectrum()
+    g32.close()
+    # per-kernel profile of the same K steps (CUDA events around every launch)
+    gp, msp, _, prof = timed_run("fp32", profile=True)
+    launches = sum(v[0] for k, v in prof.items())
+    gp.close()
+    dom = max((k for k in prof if algorithmic_bytes(k, Np, Nc, False)), key=lambda k: prof[k][1])
+    dom_ms = prof[dom][1] / prof[dom][0]
+    ab = algorithmic_bytes(dom, Np, Nc, False)
+    roof = {"kernel": dom, "bound": "hbm", "achieved": ab / (dom_ms * 1e-3) / 1e9, "peak": hbm,
+            "unit": "GB/s", "peak_source": hbm_src, "traffic": None,
+            "algorithmic_bytes_per_launch": ab, "ms_per_launch": dom_ms}
+    roof["frac"] = roof["achieved"] / hbm
+    step_bytes = 60 * Np + 24 * Nc
+    kernels = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(
+        x[1] for x in prof.values())), 4)} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+    # FP64 comparison path and the P(k) error of FP32 vs FP64
+    fp64 = None
+    if not args.no_fp64:
+        g64, ms64, _, _ = timed_run("fp64")
+        ms64 = max_over_ranks(ms64, dist)
+        k64, P64, _ = g64.power_spectrum()
+        g64.close()
+        m = (cnt > 0) & (np.arange(len(cnt)) > 0)
+        err = float(np.max(np.abs(P32[m] - P64[m]) / P64[m]))
+        fp64 = {"value": world * Np * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
+                "pk_max_rel_err_fp32_vs_fp64": err, "fp32_speedup": ms64 / ms32}
+
+    # end-to-end through the C ABI with host buffers: phi in, X and P out
+    ph = torch.from_numpy(phi).pin_memory().numpy()
+    Xh = torch.empty((Np, 3), dtype=torch.float64).pin_memory().numpy()
+    Ph = torch.empty((Np, 3), dtype=torch.float64).pin_memory().numpy()
+    g = cb.Gravity(3, n, f, L_BOX, precision="fp32", device=dev)
+    g.run(ph, A0, DA, args.warmup)
+    barrier(dist)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.run(ph, A0, DA, args.steps)
+    g.state_into(Xh, Ph)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    g.close()
+
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        try:
+            from conan_b200 import autograd as ag
+            adjoint = ag.benchmark_adjoint_ratio(device=dev)
+        except (ImportError, AttributeError, NotImplementedError):
+            adjoint = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference()
+
+    if rank == 0:
+        value = world * Np * args.steps / (ms32 * 1e-3)
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Philox white noise, scale-free GRF, Zel'dovich start)",
+            "config": {"workload": workload_name(mbits, f), "particles": Np, "mesh_cells": Nc, "L": L_BOX,
+                       "ns": NS, "a0": A0, "da": DA, "precision": "fp32 (lattice index + fp32 displacement)",
+                       "gradient": "fd4", "l2": "inputs larger than L2 (3.2 GB particle state), no flush",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roof,
+            "step_roofline": {"achieved": step_bytes * args.steps / (ms32 * 1e-3) / 1e9, "peak": hbm,
+                              "unit": "GB/s", "frac": step_bytes * args.steps / (ms32 * 1e-3) / 1e9 / hbm,
+                              "algorithmic_bytes_per_step": step_bytes},
+            "kernels": kernels,
+            "gpu_launches": launches,
+            "fp64_gpu": fp64,
+            "adjoint": adjoint,
+            "e2e": {"value": world * Np * args.steps / e2e_s, "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": phi.nbytes / args.steps,
+                    "d2h_bytes_per_step": (Xh.nbytes + Ph.nbytes) / args.steps,
+                    "what": "conan_pm_run (potential upload, Zel'dovich init, K steps) + conan_pm_get_state"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,27 @@
+"""conan_b200 -- B200-native particle-mesh step and initial conditions of conan.
+
+The compute path is libconan_pm.so (CUDA sm_100a, C ABI in include/conan_pm.h);
+this package is its Python mirror. Importing it loads the library and fails
+loudly if the library has not been built (``python -m conan_b200.build``).
+"""
+from . import _lib
+from ._lib import ConanError
+
+_lib.lib()  # fail at import time if the native library is missing
+
+from .pm import (  # noqa: E402
+    Cosmology,
+    Gravity,
+    LeapFrog,
+    compute_displacement,
+    compute_potential,
+    generate_random_field,
+    ic_params,
+    white_noise,
+)
+from .conanfile import ConanFile  # noqa: E402
+
+__all__ = [
+    "ConanError", "ConanFile", "Cosmology", "Gravity", "LeapFrog", "compute_displacement",
+    "compute_potential", "generate_random_field", "ic_params", "white_noise",
+]

@@ -1,0 +1,656 @@
+// pm.cu -- the particle-mesh solver handle (conan_pm_*), the B200
+// replacement of the reference's Gravity<R> solver (src/run/nbody.hh:53-219)
+// driven by LeapFrog::run (src/run/leapfrog.hh:33-46).
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "fft.cuh"
+#include "pm.cuh"
+
+namespace conan {
+
+std::string &last_error() {
+    static thread_local std::string s;
+    return s;
+}
+
+int set_error(int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    last_error() = buf;
+    return code;
+}
+
+double adot(double H0, double Om, double OL, double a) {
+    // Cosmology::operator(), src/run/cosmology.hh:16-23.
+    double Ok = 1 - Om - OL;
+    return H0 * a * std::sqrt(OL + Om * std::pow(a, -3) + Ok * std::pow(a, -2));
+}
+
+int check_pm_params(const conan_pm_params *p) {
+    if (!p) return set_error(CONAN_ERR_ARG, "null parameters");
+    if (p->dim < 1 || p->dim > 3)
+        return set_error(CONAN_ERR_UNSUPPORTED, "dim = %d: the GPU path supports 1, 2 and 3 dimensions",
+                         p->dim);
+    if (!is_pow2(p->n_mass) || p->n_mass < 2)
+        return set_error(CONAN_ERR_ARG, "n_mass = %d must be a power of two >= 2", p->n_mass);
+    if (!is_pow2(p->f)) return set_error(CONAN_ERR_ARG, "f = %d must be a power of two >= 1", p->f);
+    long long nf = (long long)p->n_mass * p->f;
+    long long cells = 1;
+    for (int i = 0; i < p->dim; ++i) cells *= nf;
+    if (cells >= (1LL << 32))
+        return set_error(CONAN_ERR_ARG, "force mesh of %lld cells exceeds 2^32 - 1", cells);
+    if (!(p->size > 0)) return set_error(CONAN_ERR_ARG, "box size must be positive");
+    if (p->precision != CONAN_FP32 && p->precision != CONAN_FP64)
+        return set_error(CONAN_ERR_ARG, "precision must be CONAN_FP32 or CONAN_FP64");
+    if (p->gradient != CONAN_GRAD_FD4 && p->gradient != CONAN_GRAD_SPECTRAL)
+        return set_error(CONAN_ERR_ARG, "gradient must be CONAN_GRAD_FD4 or CONAN_GRAD_SPECTRAL");
+    if (!(p->H0 > 0)) return set_error(CONAN_ERR_ARG, "H0 must be positive");
+    return CONAN_OK;
+}
+
+int device_guard(int dev) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return set_error(CONAN_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (dev < 0 || dev >= n) return set_error(CONAN_ERR_ARG, "device %d out of range (%d devices)", dev, n);
+    CONAN_CUDA(cudaSetDevice(dev));
+    return CONAN_OK;
+}
+
+// ------------------------------------------------------------------ PM --
+
+template <typename T, int R> struct PM : PMBase {
+    typedef typename Cplx<T>::type CT;
+    typedef typename Pay<T>::elem PE;
+
+    conan_pm_params prm{};
+    Mesh mf{}, mm{};
+    size_t np = 0;
+    double res_f = 0, res_m = 0, mass = 1, G = 0;
+    Parts<T> P{};
+    T *mesh = nullptr;
+    T *gm[3] = {nullptr, nullptr, nullptr};
+    CT *spec = nullptr, *spec2 = nullptr;
+    uint32_t *count = nullptr, *off = nullptr, *rank = nullptr, *bsum = nullptr;
+    int *err = nullptr;  // device error word set by kernel self-checks
+    PE *pay = nullptr;
+    double *xfer = nullptr;
+    size_t xfer_n = 0;
+    void *work = nullptr;
+    FFTPair fft;
+    cudaStream_t st = nullptr;
+    Profiler prof;
+    std::vector<void *> allocs;
+    double a_pos = 0, a_mom = 0;
+    bool ranks_pending = false;
+    int mesh_holds = 0;  // 0 nothing, 1 delta, 2 phi
+    unsigned cb_every = 1;
+    size_t bytes = 0;
+
+    ~PM() override {
+        if (st) cudaStreamSynchronize(st);
+        fft.destroy();
+        for (void *p : allocs) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    template <typename U> int alloc(U **p, size_t n) {
+        void *q = nullptr;
+        size_t b = n * sizeof(U);
+        if (b == 0) b = 16;
+        cudaError_t e = cudaMalloc(&q, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(CONAN_ERR_ALLOC, "cudaMalloc of %zu bytes failed: %s", b, cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += b;
+        *p = (U *)q;
+        return CONAN_OK;
+    }
+
+    int create(const conan_pm_params &p) {
+        prm = p;
+        int nf = p.n_mass * p.f;
+        mf = make_mesh(R, nf);
+        mm = make_mesh(R, p.n_mass);
+        np = mm.cells;
+        res_f = p.size / nf;
+        res_m = p.size / p.n_mass;
+        mass = std::pow(double(nf) / p.n_mass, R);  // src/run/nbody.hh:85
+        G = 3. / 2 * p.Omega_m * p.H0 * p.H0;       // src/run/cosmology.hh:13
+        CONAN_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        P.np = np;
+        P.mshift = mm.shift;
+        P.f = p.f;
+        for (int k = 0; k < R; ++k) {
+            CONAN_TRY(alloc(&P.d[k], np));
+            CONAN_TRY(alloc(&P.p[k], np));
+        }
+        CONAN_TRY(alloc(&mesh, mf.cells));
+        CONAN_TRY(alloc(&spec, mf.spec));
+        if (p.gradient == CONAN_GRAD_SPECTRAL) {
+            CONAN_TRY(alloc(&spec2, mf.spec));
+            for (int k = 0; k < R; ++k) CONAN_TRY(alloc(&gm[k], mf.cells));
+        }
+        CONAN_TRY(alloc(&count, mf.cells));
+        CONAN_TRY(alloc(&off, mf.cells + 1));
+        CONAN_TRY(alloc(&rank, np));
+        size_t nb = (mf.cells + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        CONAN_TRY(alloc(&bsum, nb));
+        CONAN_TRY(alloc(&pay, np * Pay<T>::words));
+        CONAN_TRY(alloc(&err, 1));
+        CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+        CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        CONAN_TRY(fft.create(mf, sizeof(T) == 8, 1));
+        CONAN_TRY(alloc((char **)&work, fft.work_bytes));
+        CONAN_TRY(fft.bind(work, st));
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return CONAN_OK;
+    }
+
+    int ensure_xfer(size_t n) {
+        if (xfer_n >= n) return CONAN_OK;
+        if (xfer) {
+            CONAN_CUDA(cudaStreamSynchronize(st));
+            for (auto it = allocs.begin(); it != allocs.end(); ++it)
+                if (*it == xfer) {
+                    allocs.erase(it);
+                    break;
+                }
+            cudaFree(xfer);
+            bytes -= xfer_n * sizeof(double);
+            xfer = nullptr;
+        }
+        CONAN_TRY(alloc(&xfer, n));
+        xfer_n = n;
+        return CONAN_OK;
+    }
+
+    dim3 grid_p() const { return dim3((unsigned)((np + 255) / 256)); }
+
+    // --- deposit ---------------------------------------------------------
+    int rank_pass() {
+        if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        CONAN_TIMED(prof, "rank", st, (k_rank<T, R><<<grid_p(), 256, 0, st>>>(P, mf, count, rank)));
+        ranks_pending = true;
+        return CONAN_OK;
+    }
+
+    int deposit() {
+        if (!ranks_pending) CONAN_TRY(rank_pass());
+        size_t nb = (mf.cells + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        CONAN_TIMED(prof, "scan", st,
+                    (k_scan_partial<<<(unsigned)nb, SCAN_T, 0, st>>>(count, mf.cells, bsum)));
+        CONAN_TIMED(prof, "scan", st, (k_scan_blocks<<<1, 1024, 0, st>>>(bsum, (int)nb)));
+        CONAN_TIMED(prof, "scan", st,
+                    (k_scan_final<<<(unsigned)nb, SCAN_T, 0, st>>>(count, mf.cells, bsum, off)));
+        ranks_pending = false;
+        CONAN_TIMED(prof, "scatter", st,
+                    (k_scatter<T, R><<<grid_p(), 256, 0, st>>>(P, mf, off, rank, pay, nullptr)));
+        double scale = mass;
+        if (mf.n >= 32) {
+            constexpr int YW = R == 3 ? 8 : 16, ZC = R == 3 ? 16 : 1, WPB = 8;
+            long long tasks = (long long)(mf.n / 32) * (R >= 2 ? mf.n / YW : 1) * (R == 3 ? mf.n / ZC : 1);
+            unsigned blocks = (unsigned)((tasks + WPB - 1) / WPB);
+            CONAN_TIMED(prof, "deposit", st,
+                        (k_deposit<T, R, YW, ZC, WPB><<<blocks, WPB * 32, 0, st>>>(off, pay, mesh, mf, scale, (uint32_t)np, err)));
+        } else {
+            CONAN_TIMED(prof, "deposit", st,
+                        (k_deposit_pull<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(
+                            off, pay, mesh, mf, scale)));
+        }
+        mesh_holds = 1;
+        return CONAN_OK;
+    }
+
+    // --- Poisson: mesh (delta) -> mesh (phi) [and gradient meshes] ------
+    int poisson(double a) {
+        double gs = -G / (a * (double)mf.cells) * std::pow(prm.size / (2 * M_PI), 2);
+        unsigned gb = (unsigned)((mf.spec + 255) / 256);
+        CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
+        CONAN_TIMED(prof, "green", st, (k_green<T><<<gb, 256, 0, st>>>(spec, mf, (T)gs)));
+        if (prm.gradient == CONAN_GRAD_SPECTRAL) {
+            for (int k = 0; k < R; ++k) {
+                CONAN_TIMED(prof, "spec_deriv", st, (k_spec_deriv<T><<<gb, 256, 0, st>>>(spec, spec2, mf, k)));
+                CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec2, gm[k])));
+            }
+        }
+        CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec, mesh)));
+        mesh_holds = 2;
+        return CONAN_OK;
+    }
+
+    int gkd(bool kick, double ck, bool drift, double cd, bool rank_after) {
+        if (rank_after && ranks_pending)
+            CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        GKD c{ck, cd, kick ? 1 : 0, drift ? 1 : 0, rank_after ? 1 : 0, prm.periodic_gather ? 1 : 0};
+        const char *name = kick ? (drift ? "gather_kick_drift" : "gather_kick") : "drift";
+        if (prm.gradient == CONAN_GRAD_SPECTRAL)
+            CONAN_TIMED(prof, name, st,
+                        (k_gkd<T, R, true><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], c,
+                                                                     count, rank)));
+        else
+            CONAN_TIMED(prof, name, st,
+                        (k_gkd<T, R, false><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], c,
+                                                                      count, rank)));
+        if (rank_after) ranks_pending = true;
+        return CONAN_OK;
+    }
+
+    double coef_drift(double a, double da) const {
+        return da / (a * a * adot(prm.H0, prm.Omega_m, prm.Omega_L, a));
+    }
+    double coef_kick(double a, double da) const {
+        return (da / adot(prm.H0, prm.Omega_m, prm.Omega_L, a)) / (res_f * res_f);
+    }
+
+    // --- API ---------------------------------------------------------------
+    int init(const double *phi, double apos, double amom) override {
+        if (!phi) return set_error(CONAN_ERR_ARG, "null potential");
+        CONAN_TRY(ensure_xfer(mm.cells));
+        CONAN_CUDA(cudaMemcpyAsync(xfer, phi, mm.cells * sizeof(double), cudaMemcpyHostToDevice, st));
+        unsigned gb = (unsigned)((mm.cells + 255) / 256);
+        CONAN_TIMED(prof, "convert", st, (k_convert<double, T><<<gb, 256, 0, st>>>(xfer, mesh, mm.cells, 1.0, 0.0)));
+        double cdz = -apos / (res_m * res_f), cpz = -amom / (res_m * res_f);
+        CONAN_TIMED(prof, "zeldovich", st, (k_zeldovich<T, R><<<grid_p(), 256, 0, st>>>(P, mesh, mm, cdz, cpz)));
+        if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        ranks_pending = false;
+        mesh_holds = 0;
+        a_pos = apos;
+        a_mom = amom;
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return CONAN_OK;
+    }
+
+    int drift(double a, double da) override {
+        CONAN_TRY(gkd(false, 0, true, coef_drift(a, da), true));
+        a_pos = a;
+        return CONAN_OK;
+    }
+
+    int kick(double a, double da) override {
+        CONAN_TRY(deposit());
+        CONAN_TRY(poisson(a));
+        CONAN_TRY(gkd(true, coef_kick(a, da), false, 0, false));
+        a_mom = a;
+        return CONAN_OK;
+    }
+
+    // Steps [i0, i1) of a leapfrog run starting at a(i0) = a; the first
+    // drift is separate, every later drift is fused into the previous kick.
+    int steps(double &a, double da, unsigned i0, unsigned i1) {
+        CONAN_TRY(gkd(false, 0, true, coef_drift(a, da), true));
+        a_pos = a;
+        for (unsigned i = i0; i < i1; ++i) {
+            double am = a + da / 2;
+            CONAN_TRY(deposit());
+            CONAN_TRY(poisson(am));
+            bool last = i + 1 == i1;
+            double an = a + da;
+            CONAN_TRY(gkd(true, coef_kick(am, da), !last, last ? 0 : coef_drift(an, da), !last));
+            a_mom = am;
+            a = an;
+            if (!last) a_pos = a;
+        }
+        return CONAN_OK;
+    }
+
+    int run(conan_pm *h, const double *phi, double a0, double da, unsigned n, conan_step_cb cb,
+            void *user) override {
+        if (phi) CONAN_TRY(init(phi, a0, a0 + da / 2));
+        double a = a0;
+        unsigned i = 0;
+        while (i < n) {
+            unsigned seg_end = n;
+            if (cb) {
+                unsigned k = cb_every ? cb_every : 1;
+                seg_end = ((i / k) + 1) * k;
+                if (seg_end > n) seg_end = n;
+            }
+            if (!prof.on && !debug_sync()) {
+                cudaGraph_t g = nullptr;
+                CONAN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                int rc = steps(a, da, i, seg_end);
+                cudaError_t ce = cudaStreamEndCapture(st, &g);
+                if (rc != CONAN_OK) {
+                    if (g) cudaGraphDestroy(g);
+                    return rc;
+                }
+                if (ce != cudaSuccess)
+                    return set_error(CONAN_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+                cudaGraphExec_t ex = nullptr;
+                cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess)
+                    return set_error(CONAN_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
+                cudaError_t le = cudaGraphLaunch(ex, st);
+                cudaError_t se = cudaStreamSynchronize(st);
+                cudaGraphExecDestroy(ex);
+                if (le != cudaSuccess)
+                    return set_error(CONAN_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(le));
+                if (se != cudaSuccess)
+                    return set_error(CONAN_ERR_CUDA, "graph execution failed: %s", cudaGetErrorString(se));
+            } else {
+                CONAN_TRY(steps(a, da, i, seg_end));
+            }
+            i = seg_end;
+            if (cb) {
+                CONAN_CUDA(cudaStreamSynchronize(st));
+                if (cb(h, i - 1, a, user) != 0)
+                    return set_error(CONAN_ERR_STATE, "step callback stopped the run after step %u", i - 1);
+            }
+        }
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return check_err();
+    }
+
+    // Reads and clears the kernels' self-check word.
+    int check_err() {
+        int h = 0;
+        CONAN_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        if (h) return set_error(CONAN_ERR_STATE, "kernel self-check failed (code %d): corrupt cell offsets", h);
+        return CONAN_OK;
+    }
+
+    int get_state(double *X, double *Pm) override {
+        CONAN_TRY(ensure_xfer(np * R));
+        for (int which = 0; which < 2; ++which) {
+            double *dst = which == 0 ? X : Pm;
+            if (!dst) continue;
+            CONAN_TIMED(prof, "export", st,
+                        (k_export<T, R><<<grid_p(), 256, 0, st>>>(P, res_f, which == 0 ? xfer : nullptr,
+                                                                  which == 1 ? xfer : nullptr)));
+            CONAN_CUDA(cudaMemcpyAsync(dst, xfer, np * R * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CONAN_CUDA(cudaStreamSynchronize(st));
+        }
+        return CONAN_OK;
+    }
+
+    int set_state(const double *X, const double *Pm, double apos, double amom) override {
+        if (!X || !Pm) return set_error(CONAN_ERR_ARG, "null state");
+        size_t n = np * R;
+        CONAN_TRY(ensure_xfer(2 * n));
+        CONAN_CUDA(cudaMemcpyAsync(xfer, X, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CONAN_CUDA(cudaMemcpyAsync(xfer + n, Pm, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        CONAN_TIMED(prof, "import", st, (k_import<T, R><<<grid_p(), 256, 0, st>>>(P, res_f, xfer, xfer + n)));
+        if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        ranks_pending = false;
+        a_pos = apos;
+        a_mom = amom;
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return CONAN_OK;
+    }
+
+    int mesh_out(double *out) {
+        CONAN_TRY(ensure_xfer(mf.cells));
+        unsigned gb = (unsigned)((mf.cells + 255) / 256);
+        CONAN_TIMED(prof, "convert", st, (k_convert<T, double><<<gb, 256, 0, st>>>(mesh, xfer, mf.cells, 1.0, 0.0)));
+        CONAN_CUDA(cudaMemcpyAsync(out, xfer, mf.cells * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return CONAN_OK;
+    }
+
+    int density(double *out) override {
+        CONAN_TRY(deposit());
+        return mesh_out(out);
+    }
+
+    int potential(double *out) override {
+        if (mesh_holds != 2) return set_error(CONAN_ERR_STATE, "no potential: call kick first");
+        return mesh_out(out);
+    }
+
+    int power_spectrum(int nbins, double *k, double *Pk, double *cnt) override {
+        if (nbins < 1) return set_error(CONAN_ERR_ARG, "nbins must be positive");
+        CONAN_TRY(deposit());
+        CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
+        mesh_holds = 1;
+        return spectrum_bins<T>(spec, mf, prm.size, nbins, k, Pk, cnt, st, this);
+    }
+
+    int scale_factors(double *ap, double *am) override {
+        if (ap) *ap = a_pos;
+        if (am) *am = a_mom;
+        return CONAN_OK;
+    }
+    int set_profiling(int on) override {
+        prof.on = on != 0;
+        return CONAN_OK;
+    }
+    int profile_entry(int i, char *name, int *launches, double *ms) override {
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        CONAN_TRY(prof.collect());
+        if (i < 0 || i >= (int)prof.names.size()) return set_error(CONAN_ERR_ARG, "no profile entry %d", i);
+        if (name) {
+            std::strncpy(name, prof.names[i].c_str(), 63);
+            name[63] = 0;
+        }
+        if (launches) *launches = prof.launches[i];
+        if (ms) *ms = prof.total_ms[i];
+        return CONAN_OK;
+    }
+    int profile_reset() override {
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        CONAN_TRY(prof.collect());
+        prof.reset();
+        return CONAN_OK;
+    }
+    int device_bytes(size_t *b) override {
+        *b = bytes + fft.work_bytes * 0;
+        return CONAN_OK;
+    }
+    int sync() override {
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return CONAN_OK;
+    }
+    int set_cb_every(unsigned k) override {
+        cb_every = k ? k : 1;
+        return CONAN_OK;
+    }
+    int device() const override { return prm.device; }
+    void *stream() const override { return (void *)st; }
+};
+
+// Power-spectrum bins from a half spectrum (deterministic two-level sum).
+__global__ void k_pk_final(const double *__restrict__ part, int nblocks, int nbins, double L, int R,
+                           double ncells, double *__restrict__ out) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= 3 * nbins) return;
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * 3 * nbins + j];
+    out[j] = s;
+}
+
+template <typename T>
+int spectrum_bins(const typename Cplx<T>::type *spec, const Mesh &m, double L, int nbins, double *k,
+                  double *Pk, double *cnt, cudaStream_t st, PMBase *) {
+    const int threads = 256, nblocks = 148 * 2;
+    size_t sh = (size_t)(threads / 32) * 3 * nbins * sizeof(double);
+    if (sh > 200 * 1024) return set_error(CONAN_ERR_ARG, "too many bins (%d)", nbins);
+    double *part = nullptr, *out = nullptr;
+    CONAN_CUDA(cudaMallocAsync((void **)&part, (size_t)nblocks * 3 * nbins * sizeof(double), st));
+    CONAN_CUDA(cudaMallocAsync((void **)&out, 3 * (size_t)nbins * sizeof(double), st));
+    if (sh > 48 * 1024)
+        CONAN_CUDA(cudaFuncSetAttribute(k_pk_partial<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    k_pk_partial<T><<<nblocks, threads, sh, st>>>(spec, m, nbins, part);
+    CONAN_LAUNCHED();
+    k_pk_final<<<(3 * nbins + 255) / 256, 256, 0, st>>>(part, nblocks, nbins, L, m.R, (double)m.cells, out);
+    CONAN_LAUNCHED();
+    std::vector<double> h(3 * (size_t)nbins);
+    CONAN_CUDA(cudaMemcpyAsync(h.data(), out, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CONAN_CUDA(cudaFreeAsync(part, st));
+    CONAN_CUDA(cudaFreeAsync(out, st));
+    CONAN_CUDA(cudaStreamSynchronize(st));
+    double norm = std::pow(L, m.R) / ((double)m.cells * (double)m.cells);
+    for (int b = 0; b < nbins; ++b) {
+        double c = h[2 * nbins + b];
+        if (cnt) cnt[b] = c;
+        if (k) k[b] = c > 0 ? h[nbins + b] / c * 2 * M_PI / L : 0;
+        if (Pk) Pk[b] = c > 0 ? h[b] / c * norm : 0;
+    }
+    return CONAN_OK;
+}
+
+template int spectrum_bins<float>(const cufftComplex *, const Mesh &, double, int, double *, double *,
+                                  double *, cudaStream_t, PMBase *);
+template int spectrum_bins<double>(const cufftDoubleComplex *, const Mesh &, double, int, double *,
+                                   double *, double *, cudaStream_t, PMBase *);
+
+PMBase *make_pm(const conan_pm_params &p) {
+    PMBase *b = nullptr;
+    int rc = CONAN_OK;
+#define MAKE(T, R)                     \
+    {                                  \
+        auto *x = new PM<T, R>();      \
+        rc = x->create(p);             \
+        b = x;                         \
+    }
+    if (p.precision == CONAN_FP32) {
+        if (p.dim == 1) MAKE(float, 1) else if (p.dim == 2) MAKE(float, 2) else MAKE(float, 3)
+    } else {
+        if (p.dim == 1) MAKE(double, 1) else if (p.dim == 2) MAKE(double, 2) else MAKE(double, 3)
+    }
+#undef MAKE
+    if (rc != CONAN_OK) {
+        std::string msg = last_error();
+        delete b;
+        last_error() = msg;
+        return nullptr;
+    }
+    return b;
+}
+
+}  // namespace conan
+
+using namespace conan;
+
+struct conan_pm {
+    PMBase *impl;
+};
+
+#define H_GUARD(h)                                                       \
+    do {                                                                 \
+        if (!(h) || !(h)->impl) return set_error(CONAN_ERR_ARG, "null handle"); \
+        CONAN_TRY(device_guard((h)->impl->device()));                    \
+    } while (0)
+
+extern "C" {
+
+const char *conan_last_error(void) { return last_error().c_str(); }
+const char *conan_version(void) { return "conan_b200 1.0 (sm_100a)"; }
+
+int conan_device_count(int *n) {
+    if (!n) return set_error(CONAN_ERR_ARG, "null pointer");
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        cudaGetLastError();
+        c = 0;
+    }
+    *n = c;
+    return CONAN_OK;
+}
+
+conan_pm *conan_pm_create(const conan_pm_params *p) {
+    last_error().clear();
+    if (check_pm_params(p) != CONAN_OK) return nullptr;
+    if (device_guard(p->device) != CONAN_OK) return nullptr;
+    PMBase *b = make_pm(*p);
+    if (!b) return nullptr;
+    return new conan_pm{b};
+}
+
+void conan_pm_destroy(conan_pm *h) {
+    if (!h) return;
+    if (h->impl) {
+        cudaSetDevice(h->impl->device());
+        delete h->impl;
+    }
+    delete h;
+}
+
+int conan_pm_init(conan_pm *h, const double *phi, double a_pos, double a_mom) {
+    H_GUARD(h);
+    return h->impl->init(phi, a_pos, a_mom);
+}
+int conan_pm_drift(conan_pm *h, double a, double da) {
+    H_GUARD(h);
+    return h->impl->drift(a, da);
+}
+int conan_pm_kick(conan_pm *h, double a, double da) {
+    H_GUARD(h);
+    return h->impl->kick(a, da);
+}
+int conan_pm_set_callback_interval(conan_pm *h, unsigned k) {
+    H_GUARD(h);
+    return h->impl->set_cb_every(k);
+}
+int conan_pm_run(conan_pm *h, const double *phi, double a0, double da, unsigned n, conan_step_cb cb,
+                 void *user) {
+    H_GUARD(h);
+    return h->impl->run(h, phi, a0, da, n, cb, user);
+}
+int conan_pm_get_state(conan_pm *h, double *X, double *P) {
+    H_GUARD(h);
+    return h->impl->get_state(X, P);
+}
+int conan_pm_set_state(conan_pm *h, const double *X, const double *P, double a_pos, double a_mom) {
+    H_GUARD(h);
+    return h->impl->set_state(X, P, a_pos, a_mom);
+}
+int conan_pm_scale_factors(conan_pm *h, double *a_pos, double *a_mom) {
+    H_GUARD(h);
+    return h->impl->scale_factors(a_pos, a_mom);
+}
+int conan_pm_density(conan_pm *h, double *delta_out) {
+    H_GUARD(h);
+    if (!delta_out) return set_error(CONAN_ERR_ARG, "null output");
+    return h->impl->density(delta_out);
+}
+int conan_pm_potential(conan_pm *h, double *phi_out) {
+    H_GUARD(h);
+    if (!phi_out) return set_error(CONAN_ERR_ARG, "null output");
+    return h->impl->potential(phi_out);
+}
+int conan_pm_power_spectrum(conan_pm *h, int nbins, double *k, double *P, double *count) {
+    H_GUARD(h);
+    return h->impl->power_spectrum(nbins, k, P, count);
+}
+int conan_pm_set_profiling(conan_pm *h, int enable) {
+    H_GUARD(h);
+    return h->impl->set_profiling(enable);
+}
+int conan_pm_profile_entry(conan_pm *h, int i, char *name, int *launches, double *total_ms) {
+    H_GUARD(h);
+    return h->impl->profile_entry(i, name, launches, total_ms);
+}
+int conan_pm_profile_reset(conan_pm *h) {
+    H_GUARD(h);
+    return h->impl->profile_reset();
+}
+int conan_pm_device_bytes(conan_pm *h, size_t *bytes) {
+    H_GUARD(h);
+    if (!bytes) return set_error(CONAN_ERR_ARG, "null pointer");
+    return h->impl->device_bytes(bytes);
+}
+int conan_pm_sync(conan_pm *h) {
+    H_GUARD(h);
+    return h->impl->sync();
+}
+int conan_pm_get_stream(conan_pm *h, void **stream) {
+    H_GUARD(h);
+    if (!stream) return set_error(CONAN_ERR_ARG, "null pointer");
+    *stream = h->impl->stream();
+    return CONAN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+"""ctypes wrappers of liboracle.so (FP64 CPU restatement; test infrastructure).
+
+Arrays follow the reference layout: meshes flat with axis 0 fastest,
+particle vectors (n, dim). Functions cite the reference code they restate in
+conan_oracle.cc.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+_d = C.c_double
+_lib = None
+
+
+def build():
+    """Builds liboracle.so (and _ref/ when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        _lib = C.CDLL(str(LIB))
+        _lib.oracle_adot.restype = C.c_double
+    return _lib
+
+
+def P(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def noise_mt19937(seed: int, n: int) -> np.ndarray:
+    out = np.empty(n)
+    lib().oracle_noise_mt19937(C.c_ulong(seed), C.c_size_t(n), P(out))
+    return out
+
+
+def dft(a: np.ndarray, dim: int, N: int, sign: int = -1) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    out = np.empty_like(a)
+    lib().oracle_dft(dim, N, P(a), P(out), sign)
+    return out
+
+
+def grf_scale_free(dim, mbits, L, ns, smooth, scale, sigma, noise) -> np.ndarray:
+    noise = np.ascontiguousarray(noise, dtype=np.float64)
+    out = np.empty_like(noise)
+    lib().oracle_grf_scale_free(dim, mbits, _d(L), _d(ns), int(smooth), _d(scale), _d(sigma), P(noise), P(out))
+    return out
+
+
+def grf_cdm(dim, mbits, L, Omega0, H0, ns, noise) -> np.ndarray:
+    noise = np.ascontiguousarray(noise, dtype=np.float64)
+    out = np.empty_like(noise)
+    lib().oracle_grf_cdm(dim, mbits, _d(L), _d(Omega0), _d(H0), _d(ns), P(noise), P(out))
+    return out
+
+
+def potential(dim, mbits, L, dens) -> np.ndarray:
+    out = np.array(dens, dtype=np.float64, copy=True)
+    lib().oracle_potential(dim, mbits, _d(L), P(out))
+    return out
+
+
+def displacement(dim, mbits, L, pot) -> np.ndarray:
+    pot = np.ascontiguousarray(pot, dtype=np.float64)
+    out = np.empty((pot.size, dim))
+    lib().oracle_displacement(dim, mbits, _d(L), P(pot), P(out))
+    return out
+
+
+def zeldovich(dim, Nm, L, phi, a_pos, a_mom):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    X = np.empty((phi.size, dim))
+    Pm = np.empty((phi.size, dim))
+    lib().oracle_zeldovich(dim, Nm, _d(L), P(phi), _d(a_pos), _d(a_mom), P(X), P(Pm))
+    return X, Pm
+
+
+def md_cic(dim, N, L, X, m=1.0) -> np.ndarray:
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.empty(N ** dim)
+    lib().oracle_md_cic(dim, N, _d(L), P(X), C.c_size_t(X.size // dim), _d(m), P(out))
+    return out
+
+
+def poisson(dim, N, L, G, a, delta_plus_one) -> np.ndarray:
+    out = np.array(delta_plus_one, dtype=np.float64, copy=True)
+    lib().oracle_poisson(dim, N, _d(L), _d(G), _d(a), P(out))
+    return out
+
+
+def interp_gradient(dim, N, L, phi, X) -> np.ndarray:
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.empty_like(X)
+    lib().oracle_interp_gradient(dim, N, _d(L), P(phi), P(X), C.c_size_t(X.size // dim), P(out))
+    return out
+
+
+def adot(H0, Om, OL, a) -> float:
+    return lib().oracle_adot(_d(H0), _d(Om), _d(OL), _d(a))
+
+
+def kick(dim, Nm, f, L, H0, Om, OL, X, Pm, a, da, want_phi=False):
+    phi = np.empty((Nm * f) ** dim) if want_phi else None
+    lib().oracle_kick(dim, Nm, f, _d(L), _d(H0), _d(Om), _d(OL), P(X), P(Pm), _d(a), _d(da),
+                      P(phi) if want_phi else None)
+    return phi
+
+
+def drift(dim, Nm, H0, Om, OL, X, Pm, a, da):
+    lib().oracle_drift(dim, Nm, _d(H0), _d(Om), _d(OL), P(X), P(Pm), _d(a), _d(da))
+
+
+def run(dim, Nm, f, L, H0, Om, OL, phi, a0, da, n):
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    X = np.empty((Nm ** dim, dim))
+    Pm = np.empty((Nm ** dim, dim))
+    lib().oracle_run(dim, Nm, f, _d(L), _d(H0), _d(Om), _d(OL), P(phi), _d(a0), _d(da), C.c_uint(n), P(X), P(Pm))
+    return X, Pm
+
+
+def power_spectrum(dim, N, L, delta, nbins=None):
+    nb = nbins or N // 2 + 1
+    delta = np.ascontiguousarray(delta, dtype=np.float64)
+    k, p, c = np.empty(nb), np.empty(nb), np.empty(nb)
+    lib().oracle_power_spectrum(dim, N, _d(L), P(delta), nb, P(k), P(p), P(c))
+    return k, p, c
