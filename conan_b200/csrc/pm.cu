@@ -77,6 +77,7 @@ template <typename T, int R> struct PM : PMBase {
     Parts<T> P{};
     T *mesh = nullptr;
     T *gm[3] = {nullptr, nullptr, nullptr};
+    G4<T> *grad = nullptr;  // packed FD4 gradient mesh
     CT *spec = nullptr, *spec2 = nullptr;
     uint32_t *count = nullptr, *off = nullptr, *rank = nullptr, *bsum = nullptr;
     int *err = nullptr;  // device error word set by kernel self-checks
@@ -139,6 +140,8 @@ template <typename T, int R> struct PM : PMBase {
         if (p.gradient == CONAN_GRAD_SPECTRAL) {
             CONAN_TRY(alloc(&spec2, mf.spec));
             for (int k = 0; k < R; ++k) CONAN_TRY(alloc(&gm[k], mf.cells));
+        } else {
+            CONAN_TRY(alloc(&grad, mf.cells));
         }
         CONAN_TRY(alloc(&count, mf.cells));
         CONAN_TRY(alloc(&off, mf.cells + 1));
@@ -196,12 +199,15 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TIMED(prof, "scatter", st,
                     (k_scatter<T, R><<<grid_p(), 256, 0, st>>>(P, mf, off, rank, pay, nullptr)));
         double scale = mass;
-        if (mf.n >= 32) {
-            constexpr int YW = R == 3 ? 8 : 16, ZC = R == 3 ? 16 : 1, WPB = 8;
-            long long tasks = (long long)(mf.n / 32) * (R >= 2 ? mf.n / YW : 1) * (R == 3 ? mf.n / ZC : 1);
-            unsigned blocks = (unsigned)((tasks + WPB - 1) / WPB);
+        typedef DepTile<R> D;
+        if (mf.n >= D::TX && mf.n >= D::TY && mf.n >= D::TZ) {
+            size_t tiles = (size_t)(mf.n / D::TX) * (R >= 2 ? mf.n / D::TY : 1) * (R == 3 ? mf.n / D::TZ : 1);
+            constexpr size_t sh = deposit_smem<T, R>();
+            auto kern = k_deposit<T, R, D::TX, D::TY, D::TZ, D::THREADS>;
+            if (sh > 48 * 1024)
+                CONAN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
             CONAN_TIMED(prof, "deposit", st,
-                        (k_deposit<T, R, YW, ZC, WPB><<<blocks, WPB * 32, 0, st>>>(off, pay, mesh, mf, scale, (uint32_t)np, err)));
+                        (kern<<<(unsigned)tiles, D::THREADS, sh, st>>>(off, pay, mesh, mf, scale, (uint32_t)np, err)));
         } else {
             CONAN_TIMED(prof, "deposit", st,
                         (k_deposit_pull<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(
@@ -224,6 +230,9 @@ template <typename T, int R> struct PM : PMBase {
             }
         }
         CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec, mesh)));
+        if (prm.gradient == CONAN_GRAD_FD4)
+            CONAN_TIMED(prof, "fd_grad", st,
+                        (k_fd_grad<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(mesh, grad, mf)));
         mesh_holds = 2;
         return CONAN_OK;
     }
@@ -235,11 +244,11 @@ template <typename T, int R> struct PM : PMBase {
         const char *name = kick ? (drift ? "gather_kick_drift" : "gather_kick") : "drift";
         if (prm.gradient == CONAN_GRAD_SPECTRAL)
             CONAN_TIMED(prof, name, st,
-                        (k_gkd<T, R, true><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], c,
+                        (k_gkd<T, R, true><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], grad, c,
                                                                      count, rank)));
         else
             CONAN_TIMED(prof, name, st,
-                        (k_gkd<T, R, false><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], c,
+                        (k_gkd<T, R, false><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], grad, c,
                                                                       count, rank)));
         if (rank_after) ranks_pending = true;
         return CONAN_OK;
@@ -373,7 +382,7 @@ template <typename T, int R> struct PM : PMBase {
             CONAN_CUDA(cudaMemcpyAsync(dst, xfer, np * R * sizeof(double), cudaMemcpyDeviceToHost, st));
             CONAN_CUDA(cudaStreamSynchronize(st));
         }
-        return CONAN_OK;
+        return check_err();
     }
 
     int set_state(const double *X, const double *Pm, double apos, double amom) override {
@@ -397,7 +406,7 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TIMED(prof, "convert", st, (k_convert<T, double><<<gb, 256, 0, st>>>(mesh, xfer, mf.cells, 1.0, 0.0)));
         CONAN_CUDA(cudaMemcpyAsync(out, xfer, mf.cells * sizeof(double), cudaMemcpyDeviceToHost, st));
         CONAN_CUDA(cudaStreamSynchronize(st));
-        return CONAN_OK;
+        return check_err();
     }
 
     int density(double *out) override {
@@ -415,7 +424,8 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TRY(deposit());
         CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
         mesh_holds = 1;
-        return spectrum_bins<T>(spec, mf, prm.size, nbins, k, Pk, cnt, st, this);
+        CONAN_TRY(spectrum_bins<T>(spec, mf, prm.size, nbins, k, Pk, cnt, st, this));
+        return check_err();
     }
 
     int scale_factors(double *ap, double *am) override {
@@ -451,7 +461,7 @@ template <typename T, int R> struct PM : PMBase {
     }
     int sync() override {
         CONAN_CUDA(cudaStreamSynchronize(st));
-        return CONAN_OK;
+        return check_err();
     }
     int set_cb_every(unsigned k) override {
         cb_every = k ? k : 1;

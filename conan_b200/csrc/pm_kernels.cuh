@@ -323,157 +323,247 @@ template <typename T, int R> __device__ inline T corner_weight(const T *fr, int 
 
 // ------------------------------------------------------ deposit reduce --
 
-// Lanes of the run of equal `cell` values containing this lane (cells are
-// nondecreasing across the warp), and whether this lane leads it.
-__device__ inline unsigned run_mask(int cell, int lane, bool *leader) {
-    int prev = __shfl_up_sync(FULL, cell, 1);
-    bool head = lane == 0 || cell != prev;
-    unsigned heads = __ballot_sync(FULL, head);
-    unsigned upto = FULL >> (31 - lane);
-    int start = 31 - __clz(heads & upto);
-    unsigned above = lane == 31 ? 0u : (heads & (FULL << (lane + 1)));
-    int end = above ? (__ffs(above) - 2) : 31;
-    *leader = lane == start;
-    unsigned hi = end == 31 ? FULL : ((1u << (end + 1)) - 1u);
-    return hi & (FULL << start);
+// Tile accumulators of the deposit: W 32-bit words per cell stored as W
+// planes of CELLS words (so lanes flushing neighbouring cells hit distinct
+// banks), updated with native 32-bit shared atomics and explicit carries.
+// FP32: 64-bit sums in units of 2^-23. FP64: 96-bit sums in units of 2^-52.
+template <typename T> struct Slot;
+template <> struct Slot<float> {
+    static constexpr int W = 2;
+    __device__ static inline void add(uint32_t *s, int c, uint32_t v, int cells) {
+        if (!v) return;
+        uint32_t old = atomicAdd(s + c, v);
+        if (old + v < old) atomicAdd(s + cells + c, 1u);
+    }
+    __device__ static inline double value(const uint32_t *s, int c, int cells) {
+        return ((double)s[cells + c] * 4294967296.0 + (double)s[c]) * 0x1p-23;
+    }
+};
+template <> struct Slot<double> {
+    static constexpr int W = 3;
+    __device__ static inline void add(uint32_t *s, int c, unsigned long long v, int cells) {
+        if (!v) return;
+        uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);  // hi < 2^31
+        uint32_t old = atomicAdd(s + c, lo);
+        uint32_t x = hi + (old + lo < old ? 1u : 0u);
+        if (!x) return;
+        uint32_t old1 = atomicAdd(s + cells + c, x);
+        if (old1 + x < old1) atomicAdd(s + 2 * cells + c, 1u);
+    }
+    __device__ static inline double value(const uint32_t *s, int c, int cells) {
+        return (double)s[2 * cells + c] * 0x1p12 + (double)s[cells + c] * 0x1p-20 + (double)s[c] * 0x1p-52;
+    }
+};
+
+// Per-thread register sums of the 2^R corner weights of one source cell.
+template <typename T> struct RegAcc;
+template <> struct RegAcc<float> {
+    typedef uint32_t type;                 // <= 2^23 per particle
+    static constexpr int max_terms = 511;  // 511 * 2^23 < 2^32
+};
+template <> struct RegAcc<double> {
+    typedef unsigned long long type;        // <= 2^52 per particle
+    static constexpr int max_terms = 2047;  // 2047 * 2^52 < 2^63
+};
+
+__device__ inline uint32_t quant_w(float w) {
+    return __float_as_uint(__fmaf_rn(w, 8388608.0f, 8388608.0f)) - 0x4B000000u;
+}
+__device__ inline unsigned long long quant_w(double w) {
+    return (unsigned long long)(__double_as_longlong(__fma_rn(w, 4503599627370496.0, 4503599627370496.0)) -
+                                0x4330000000000000LL);
 }
 
-// Segmented integer sum of the quantised weight over a run of lanes.
-__device__ inline unsigned long long run_sum(unsigned mask, uint32_t q) {
-    return __reduce_add_sync(mask, q);
-}
-__device__ inline unsigned long long run_sum(unsigned mask, unsigned long long q) {
-    uint32_t hi = (uint32_t)(q >> 26), lo = (uint32_t)(q & 0x3FFFFFFull);
-    unsigned long long sh = __reduce_add_sync(mask, hi), sl = __reduce_add_sync(mask, lo);
-    return (sh << 26) + sl;
-}
-__device__ inline void acc_add(unsigned long long &a, unsigned long long v) { a += v; }
-__device__ inline void acc_add(U128 &a, unsigned long long v) { a = a + U128{v, 0ull}; }
+// Tile shape of the deposit for dimension R: TX x TY x TZ output cells.
+template <int R> struct DepTile;
+template <> struct DepTile<3> { static constexpr int TX = 32, TY = 8, TZ = 8, THREADS = 256; };
+template <> struct DepTile<2> { static constexpr int TX = 32, TY = 32, TZ = 1, THREADS = 256; };
+template <> struct DepTile<1> { static constexpr int TX = 1024, TY = 1, TZ = 1, THREADS = 256; };
 
-// One warp deposits a strip of 32 cells along axis 0 for YW rows (R >= 2) and
-// ZC planes (R == 3): out[c] = mass * sum of corner weights - 1.
-// Requires n % 32 == 0, n % YW == 0, n % ZC == 0.
-template <typename T, int R, int YW, int ZC, int WPB>
-__global__ void __launch_bounds__(WPB * 32)
+// One CTA deposits one output tile. Its source cells are the tile plus one
+// cell on the low side of every axis (a particle in cell s reaches s..s+1).
+// The sorted particles of those source cells form (TY+1)(TZ+1) contiguous
+// row ranges; the CTA stages their cell offsets in shared memory, splits the
+// concatenated particle list into equal contiguous slices (one per thread,
+// load-balanced whatever the clustering), and each thread sums the corner
+// weights of consecutive particles of one cell in registers, flushing to the
+// tile's integer accumulators when the cell changes. Integer sums make the
+// result independent of the order of particles and flushes.
+template <typename T, int R, int TX, int TY, int TZ, int THREADS>
+__global__ void __launch_bounds__(THREADS, 4)
     k_deposit(const uint32_t *__restrict__ off, const typename Pay<T>::elem *__restrict__ pay,
               T *__restrict__ out, Mesh m, double scale, uint32_t np, int *__restrict__ err) {
-    typedef typename Acc<T>::type A;
+    constexpr int HY = R >= 2 ? 1 : 0, HZ = R == 3 ? 1 : 0;
+    constexpr int NR = (TY + HY) * (TZ + HZ);  // source rows
+    constexpr int RAW = TX + 3;                 // hb, he, off[x0 .. x0+TX]
+    constexpr int CELLS = TX * TY * TZ;
     constexpr int C = 1 << R;
-    __shared__ A slots[WPB][34][C];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    extern __shared__ __align__(16) unsigned char dep_sh[];
+    uint32_t *slot = reinterpret_cast<uint32_t *>(dep_sh);
+    uint32_t *raw = slot + Slot<T>::W * CELLS;
+    uint32_t *rp = raw + NR * RAW;  // NR + 1 row prefixes
+
     const int n = m.n, mask = n - 1;
-    const int nxs = n >> 5, nys = R >= 2 ? n / YW : 1, nzs = R == 3 ? n / ZC : 1;
-    long long task = (long long)blockIdx.x * WPB + w;
-    if (task >= (long long)nxs * nys * nzs) return;
-    const int xs = (int)(task % nxs);
-    const int ys = (int)((task / nxs) % nys);
-    const int zs = (int)(task / ((long long)nxs * nys));
-    const int x0 = xs * 32, y0 = ys * YW, z0 = zs * ZC;
+    const int ntx = n / TX, nty = R >= 2 ? n / TY : 1;
+    const int tile = blockIdx.x;
+    const int x0 = (tile % ntx) * TX;
+    const int y0 = R >= 2 ? ((tile / ntx) % nty) * TY : 0;
+    const int z0 = R == 3 ? (tile / (ntx * nty)) * TZ : 0;
     const int hx = (x0 - 1) & mask;
 
-    for (int j = lane; j < 34 * C; j += 32) (&slots[w][0][0])[j] = Acc<T>::zero();
-    __syncwarp();
+    for (int c = threadIdx.x; c < Slot<T>::W * CELLS; c += THREADS) slot[c] = 0u;
+    for (int i = threadIdx.x; i < NR * RAW; i += THREADS) {
+        int r = i / RAW, k = i % RAW;
+        int ry = r % (TY + HY), rz = r / (TY + HY);
+        int y = (y0 - HY + ry) & mask, z = (z0 - HZ + rz) & mask;
+        size_t rb = 0;
+        if (R == 2) rb = (size_t)y << m.shift;
+        if (R == 3) rb = ((size_t)z << (2 * m.shift)) | ((size_t)y << m.shift);
+        size_t idx = k == 0 ? rb + hx : k == 1 ? rb + hx + 1 : rb + x0 + (k - 2);
+        raw[i] = __ldg(off + idx);
+    }
+    __syncthreads();
 
-    A plane[YW > 0 ? YW : 1];
-#pragma unroll
-    for (int y = 0; y < (YW > 0 ? YW : 1); ++y) plane[y] = Acc<T>::zero();
-
-    const int zlo = R == 3 ? -1 : 0, zhi = R == 3 ? ZC : 1;
-    for (int zz = zlo; zz < zhi; ++zz) {
-        const int z = (z0 + zz) & mask;
-        A rowc[2] = {Acc<T>::zero(), Acc<T>::zero()};
-#pragma unroll
-        for (int yi = 0; yi < (R >= 2 ? YW + 1 : 1); ++yi) {
-            const int yy = R >= 2 ? yi - 1 : 0;
-            const int y = (y0 + yy) & mask;
-            size_t rb = 0;
-            if (R == 2) rb = (size_t)y << m.shift;
-            if (R == 3) rb = ((size_t)z << (2 * m.shift)) | ((size_t)y << m.shift);
-
-            // Cell ranges of this row: halo cell x0-1 (logical cell 0) and
-            // cells x0..x0+31 (logical cells 1..32).
-            uint32_t e = __ldg(off + rb + x0 + lane + 1);
-            uint32_t b0 = __ldg(off + rb + x0);
-            uint32_t hb = __ldg(off + rb + hx), he = __ldg(off + rb + hx + 1);
-            uint32_t hcount = he - hb;
-            uint32_t Bv = hcount + (e - b0);
-            uint32_t total = __shfl_sync(FULL, Bv, 31);
-            // Offsets are monotone by construction; never walk a corrupt range.
-            if (__any_sync(FULL, e < b0 || he < hb) || total > np) {
-                if (lane == 0) atomicOr(err, 2);
-                total = 0;
+    // Row totals (validated) and their exclusive prefix, by warp 0.
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        uint32_t run = 0;
+        for (int base = 0; base < NR; base += 32) {
+            int r = base + lane;
+            uint32_t tot = 0;
+            if (r < NR) {
+                const uint32_t *w = raw + r * RAW;
+                bool ok = w[1] >= w[0] && w[TX + 2] >= w[2];
+                tot = ok ? (w[1] - w[0]) + (w[TX + 2] - w[2]) : 0u;
+                if (!ok) atomicOr(err, 2);
             }
-
-            for (uint32_t base = 0; base < total; base += 32) {
-                uint32_t j = base + lane;
-                bool active = j < total;
-                // Binary search over the 32 cell ends held by the lanes (all
-                // lanes take part in every shuffle).
-                int pos = 0;
-#pragma unroll
-                for (int step = 16; step >= 1; step >>= 1) {
-                    uint32_t v = __shfl_sync(FULL, Bv, pos + step - 1);
-                    if (v <= j) pos += step;
-                }
-                int cell = j < hcount ? 0 : 1 + pos;
-                uint32_t src = j < hcount ? hb + j : b0 + (j - hcount);
-                if (!active) cell = 33;
-                if (active && src >= np) {  // corrupt offsets: flag, skip
-                    atomicOr(err, 1);
-                    active = false;
-                    cell = 33;
-                }
-                T fr[3] = {T(0), T(0), T(0)};
-                if (active) load_frac<T, R>(pay, src, fr);
-                bool leader;
-                unsigned rm = run_mask(cell, lane, &leader);
-#pragma unroll
-                for (int b = 0; b < C; ++b) {
-                    auto q = Acc<T>::quant(corner_weight<T, R>(fr, b));
-                    if (!active) q = 0;
-                    unsigned long long s = run_sum(rm, q);
-                    if (leader) acc_add(slots[w][cell][b], s);
-                }
-                __syncwarp();
+            uint32_t inc = tot;
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t v = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += v;
             }
-
-            // Combine the row: bx via the neighbouring slot, by via the
-            // previous row (rowc), bz via the previous plane (plane[]).
-            A t[2][2];
-#pragma unroll
-            for (int by = 0; by < 2; ++by)
-#pragma unroll
-                for (int bz = 0; bz < 2; ++bz) {
-                    t[by][bz] = Acc<T>::zero();
-                    if ((by && R < 2) || (bz && R < 3)) continue;
-                    int b = 2 * by + 4 * bz;
-                    t[by][bz] = slots[w][lane + 1][b] + slots[w][lane][b + 1];
-                }
-            __syncwarp();
-            for (int j = lane; j < 34 * C; j += 32) (&slots[w][0][0])[j] = Acc<T>::zero();
-            __syncwarp();
-
-            A o0, o1;
-            if (R >= 2) {
-                o0 = t[0][0] + rowc[0];
-                o1 = t[0][1] + rowc[1];
-                rowc[0] = t[1][0];
-                rowc[1] = t[1][1];
-            } else {
-                o0 = t[0][0];
-                o1 = Acc<T>::zero();
-            }
-            if (yy < 0) continue;
-            A tot = o0;
-            if (R == 3) {
-                tot = o0 + plane[yy];
-                plane[yy] = o1;
-            }
-            if (zz < 0) continue;
-            out[rb + x0 + lane] = (T)(Acc<T>::value(tot) * scale - 1.0);
+            if (r < NR) rp[r] = run + inc - tot;
+            run += __shfl_sync(FULL, inc, 31);
         }
+        // halo rows/columns repeat cells when a tile spans the whole mesh,
+        // so a valid total is at most 2^R times the particle count
+        bool bad = (unsigned long long)run > ((unsigned long long)np << R);
+        if (lane == 0) rp[NR] = bad ? 0u : run;
+        if (lane == 0 && bad) atomicOr(err, 2);
+    }
+    __syncthreads();
+
+    const uint32_t total = rp[NR];
+    const uint32_t P = (total + THREADS - 1) / THREADS;
+    uint32_t g = threadIdx.x * P;
+    const uint32_t gend = min(g + P, total);
+    if (g < gend) {
+        // starting row: last r with rp[r] <= g
+        int r = 0;
+        for (int step = 512; step >= 1; step >>= 1)
+            if (r + step <= NR - 1 && rp[r + step] <= g) r += step;
+        while (r < NR - 1 && rp[r + 1] <= g) ++r;
+        const uint32_t *w = raw + r * RAW;
+        uint32_t hb = w[0], hc = w[1] - w[0], b0 = w[2];
+        uint32_t j = g - rp[r];
+        uint32_t rowtot = rp[r + 1] - rp[r];
+        // logical cell m: 0 = halo x0-1, 1 + L = cell x0 + L;
+        // boundary B(m) = 0 (m = 0), hc + w[m + 1] - b0 (m >= 1)
+        int mc = 0;
+        while (mc < TX && hc + (w[mc + 2] - b0) <= j) ++mc;
+        uint32_t nb = hc + (w[mc + 2] - b0);  // end of cell mc
+        typename RegAcc<T>::type acc[C];
+#pragma unroll
+        for (int b = 0; b < C; ++b) acc[b] = 0;
+        int terms = 0;
+
+#define CONAN_DEP_FLUSH()                                                                   \
+    do {                                                                                    \
+        if (terms) {                                                                        \
+            int ry_ = r % (TY + HY), rz_ = r / (TY + HY);                                  \
+            int sx_ = mc - 1, sy_ = ry_ - HY, sz_ = rz_ - HZ;                              \
+            _Pragma("unroll") for (int b = 0; b < C; ++b) {                                 \
+                int ox = sx_ + (b & 1);                                                     \
+                int oy = R >= 2 ? sy_ + ((b >> 1) & 1) : 0;                                 \
+                int oz = R == 3 ? sz_ + ((b >> 2) & 1) : 0;                                 \
+                if (ox >= 0 && ox < TX && oy >= 0 && oy < TY && oz >= 0 && oz < TZ)         \
+                    Slot<T>::add(slot, (oz * TY + oy) * TX + ox, acc[b], CELLS);             \
+                acc[b] = 0;                                                                 \
+            }                                                                               \
+            terms = 0;                                                                      \
+        }                                                                                   \
+    } while (0)
+
+        for (; g < gend; ++g, ++j) {
+            while (j >= rowtot) {  // next non-empty row
+                CONAN_DEP_FLUSH();
+                ++r;
+                w = raw + r * RAW;
+                hb = w[0];
+                hc = w[1] - w[0];
+                b0 = w[2];
+                j = 0;
+                rowtot = rp[r + 1] - rp[r];
+                mc = 0;
+                nb = hc;
+            }
+            while (j >= nb && mc < TX) {  // next non-empty cell of the row
+                CONAN_DEP_FLUSH();
+                ++mc;
+                nb = hc + (w[mc + 2] - b0);
+            }
+            if (j >= nb) {  // non-monotone offsets: unreachable, never walk on
+                atomicOr(err, 4);
+                break;
+            }
+            uint32_t src = mc == 0 ? hb + j : b0 + (j - hc);
+            if (src >= np) {  // unreachable with valid offsets
+                atomicOr(err, 1);
+                continue;
+            }
+            T fr[3];
+            load_frac<T, R>(pay, src, fr);
+            T g0 = T(1) - fr[0];
+            T wx[2] = {g0, fr[0]};
+            T wy[2] = {T(1), T(1)}, wz[2] = {T(1), T(1)};
+            if (R >= 2) {
+                wy[0] = T(1) - fr[1];
+                wy[1] = fr[1];
+            }
+            if (R == 3) {
+                wz[0] = T(1) - fr[2];
+                wz[1] = fr[2];
+            }
+#pragma unroll
+            for (int b = 0; b < C; ++b) {
+                T wb = wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1];
+                acc[b] += quant_w(wb);
+            }
+            if (++terms == RegAcc<T>::max_terms) CONAN_DEP_FLUSH();
+        }
+        CONAN_DEP_FLUSH();
+    }
+#undef CONAN_DEP_FLUSH
+    __syncthreads();
+
+    for (int c = threadIdx.x; c < CELLS; c += THREADS) {
+        int ox = c % TX, oy = (c / TX) % TY, oz = c / (TX * TY);
+        size_t o = (size_t)(x0 + ox);
+        if (R >= 2) o |= (size_t)(y0 + oy) << m.shift;
+        if (R == 3) o |= (size_t)(z0 + oz) << (2 * m.shift);
+        out[o] = (T)(Slot<T>::value(slot, c, CELLS) * scale - 1.0);
     }
 }
+
+template <typename T, int R> constexpr size_t deposit_smem() {
+    typedef DepTile<R> D;
+    constexpr int HY = R >= 2 ? 1 : 0, HZ = R == 3 ? 1 : 0;
+    constexpr int NR = (D::TY + HY) * (D::TZ + HZ);
+    return sizeof(uint32_t) * (Slot<T>::W * D::TX * D::TY * D::TZ + NR * (D::TX + 3) + NR + 1);
+}
+
+__device__ inline void acc_add(unsigned long long &a, unsigned long long v) { a += v; }
+__device__ inline void acc_add(U128 &a, unsigned long long v) { a = a + U128{v, 0ull}; }
 
 // Reference kernel for small meshes (n < 32): one thread per output cell
 // pulls the particles of its 2^R source cells. Same integer sums.
@@ -567,11 +657,46 @@ __device__ inline void gather_axis(T d, int q, bool periodic, int *o, T *a1) {
     *a1 = fr;
 }
 
+// Packed gradient of one mesh node (x, y, z, unused).
+template <typename T> struct alignas(16) G4 {
+    T x, y, z, w;
+};
+__device__ inline G4<float> load_g4(const G4<float> *p) {
+    float4 v = __ldg(reinterpret_cast<const float4 *>(p));
+    return G4<float>{v.x, v.y, v.z, v.w};
+}
+__device__ inline G4<double> load_g4(const G4<double> *p) {
+    double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    return G4<double>{a.x, a.y, b.x, b.y};
+}
+
+// The FD4 gradient of phi at every node, in units of phi per cell, packed:
+// the reference's Gradient<R>::operator[] (src/run/numeric.hh:88-100)
+// evaluated once per node for all particles that interpolate it.
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_fd_grad(const T *__restrict__ phi, G4<T> *__restrict__ G, Mesh m) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.cells) return;
+    const uint32_t mask = m.n - 1;
+    const T c12 = T(1) / T(12), c23 = T(2) / T(3);
+    T g[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int sh = k * m.shift;
+        uint32_t ck = (c >> sh) & mask, rest = c & ~(mask << sh);
+        auto at = [&](int o) { return __ldg(phi + (rest | (((ck + o) & mask) << sh))); };
+        g[k] = (at(-2) - at(2)) * c12 + (at(1) - at(-1)) * c23;
+    }
+    G[c] = G4<T>{g[0], g[1], g[2], T(0)};
+}
+
 // CIC-interpolated force of particle i: sum over corners of weight times
-// the gradient (FD4 of phi, or the spectral gradient meshes g[k]).
+// the node gradient (packed FD4 mesh G, or the spectral gradient meshes g[k]).
 template <typename T, int R, bool SPECTRAL>
 __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, const T *phi,
-                                    const T *const *g, bool periodic, const T *d, T *F) {
+                                    const T *const *g, const G4<T> *__restrict__ G, bool periodic,
+                                    const T *d, T *F) {
     int q[3], o[3];
     T a1[3], a0[3];
     lattice<T, R>(P, i, q);
@@ -582,27 +707,56 @@ __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, 
         F[k] = T(0);
     }
     const int mask = m.n - 1;
+    if constexpr (SPECTRAL) {
 #pragma unroll
-    for (int b = 0; b < (1 << R); ++b) {
-        T z = 1;
-        int c[3];
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            int bk = (b >> k) & 1;
-            z *= bk ? a1[k] : a0[k];
-            c[k] = (o[k] + bk) & mask;
-        }
-        if constexpr (SPECTRAL) {
+        for (int b = 0; b < (1 << R); ++b) {
+            T z = 1;
             size_t ci = 0;
 #pragma unroll
-            for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (size_t)c[k];
+            for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (size_t)((o[k] + ((b >> k) & 1)) & mask);
+#pragma unroll
+            for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
 #pragma unroll
             for (int k = 0; k < R; ++k) F[k] += __ldg(g[k] + ci) * z;
-        } else {
+        }
+    } else {
+        // FD4 gradient of the corner nodes from the packed gradient mesh
+        // (one 16-byte load per corner for FP32).
+        (void)phi;
 #pragma unroll
-            for (int k = 0; k < R; ++k) F[k] += fd4<T, R>(phi, c, k, m.shift, mask) * z;
+        for (int b = 0; b < (1 << R); ++b) {
+            uint32_t ci = 0;
+#pragma unroll
+            for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
+            T z = 1;
+#pragma unroll
+            for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
+            G4<T> gv = load_g4(G + ci);
+            F[0] += gv.x * z;
+            if (R > 1) F[1] += gv.y * z;
+            if (R > 2) F[2] += gv.z * z;
         }
     }
+}
+
+// Particle index of thread `tid` of block `blk` when the lattice is walked in
+// compact tiles (16x4x4 in 3D, 32x8 in 2D) so that a block's particles,
+// and so their potential reads, stay close together; linear otherwise.
+template <typename T, int R>
+__device__ inline size_t tiled_index(const Parts<T> &P, unsigned blk, unsigned tid) {
+    const int s = P.mshift;
+    if (R == 3 && s >= 4) {
+        size_t tx = blk & ((1u << (s - 4)) - 1), rest = blk >> (s - 4);
+        size_t ty = rest & ((1u << (s - 2)) - 1), tz = rest >> (s - 2);
+        size_t x = tx * 16 + (tid & 15), y = ty * 4 + ((tid >> 4) & 3), z = tz * 4 + (tid >> 6);
+        return x | (y << s) | (z << (2 * s));
+    }
+    if (R == 2 && s >= 5) {
+        size_t tx = blk & ((1u << (s - 5)) - 1), ty = blk >> (s - 5);
+        size_t x = tx * 32 + (tid & 31), y = ty * 8 + (tid >> 5);
+        return x | (y << s);
+    }
+    return (size_t)blk * 256 + tid;
 }
 
 struct GKD {
@@ -617,9 +771,9 @@ struct GKD {
 template <typename T, int R, bool SPECTRAL>
 __global__ void __launch_bounds__(256)
     k_gkd(Parts<T> P, Mesh m, const T *__restrict__ phi, const T *__restrict__ g0,
-          const T *__restrict__ g1, const T *__restrict__ g2, GKD c, uint32_t *__restrict__ count,
-          uint32_t *__restrict__ rank) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+          const T *__restrict__ g1, const T *__restrict__ g2, const G4<T> *__restrict__ G, GKD c,
+          uint32_t *__restrict__ count, uint32_t *__restrict__ rank) {
+    size_t i = tiled_index<T, R>(P, blockIdx.x, threadIdx.x);
     if (i >= P.np) return;
     T d[3], p[3];
 #pragma unroll
@@ -630,7 +784,7 @@ __global__ void __launch_bounds__(256)
     if (c.kick) {
         T F[3];
         const T *g[3] = {g0, g1, g2};
-        gather_force<T, R, SPECTRAL>(P, m, i, phi, g, c.periodic, d, F);
+        gather_force<T, R, SPECTRAL>(P, m, i, phi, g, G, c.periodic, d, F);
         const T ck = (T)c.ck;
 #pragma unroll
         for (int k = 0; k < R; ++k) {

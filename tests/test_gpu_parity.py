@@ -65,7 +65,8 @@ def _particles(dim, Nm, f, L, amp, seed):
     return np.ascontiguousarray(X), np.ascontiguousarray(Pm)
 
 
-@pytest.mark.parametrize("dim,Nm,f", [(2, 64, 1), (3, 32, 1), (3, 16, 2), (2, 32, 2), (3, 8, 2), (1, 64, 1)])
+@pytest.mark.parametrize("dim,Nm,f", [(2, 64, 1), (3, 32, 1), (3, 16, 2), (2, 32, 2), (3, 8, 2), (1, 64, 1),
+                                      (2, 32, 1), (1, 1024, 1), (1, 512, 4), (3, 64, 1)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("fp32", 1e-5)])
 def test_deposit_matches_md_cic(gpu, conan, oracle, dim, Nm, f, prec, tol):
     L = 40.0
