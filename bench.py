@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     return ap.parse_args()
 
 
@@ -127,11 +128,12 @@ def barrier(dist):
         dist.barrier()
 
 
-def max_over_ranks(x, dist):
+def max_over_ranks(x, dist, device="cuda"):
+    """Max of x over all ranks (device "cpu" for the gloo backend)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -318,6 +320,23 @@ def run_ours(args):
         except (ImportError, AttributeError, NotImplementedError):
             adjoint = None
 
+    ensemble = None
+    if not args.no_ensemble and rank == 0:
+        from conan_b200.ensemble import Ensemble
+        e = Ensemble.standard(device=dev)
+        e.init()
+        e.run()  # warm-up: builds and instantiates the graph
+        run_ms = min(e.run() for _ in range(3))
+        e.forward_adjoint()
+        _, adj_ms = e.last_ms()
+        n_ens = e.total_particles()
+        ensemble = {"workload": "96 boxes: 32 x 32^3, 32 x 64^3, 32 x 128^3 particles = mesh, L=100, "
+                                "ns in {-2.5,-2,-1.5,-1} (default_rng(6)), seeds 1000+i, 40 steps a=0.05->1, FP32",
+                    "particles": n_ens, "run_ms": run_ms,
+                    "particle_steps_per_s": n_ens * 40 / (run_ms * 1e-3),
+                    "forward_adjoint_ms": adj_ms, "tuning": e.describe()}
+        e.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference()
@@ -341,6 +360,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "fp64_gpu": fp64,
             "adjoint": adjoint,
+            "ensemble": ensemble,
             "e2e": {"value": world * Np * args.steps / e2e_s, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": phi.nbytes / args.steps,
                     "d2h_bytes_per_step": (Xh.nbytes + Ph.nbytes) / args.steps,

@@ -60,37 +60,49 @@ inline int ilog2(long long n) {
 
 // -------------------------------------------------------------- geometry --
 
-// A periodic mesh of n^R cells, axis 0 fastest (the reference's Box<R>,
-// src/base/box.hh:26-82), and its half-complex spectrum nh x n^(R-1),
-// nh = n/2 + 1, as cuFFT lays out an R2C transform whose fastest axis is 0.
+// A batch of `batch` periodic meshes of n^R cells each, axis 0 fastest (the
+// reference's Box<R>, src/base/box.hh:26-82), stored back to back, and their
+// half-complex spectra of nh x n^(R-1) values each, nh = n/2 + 1, as cuFFT
+// lays out an R2C transform whose fastest axis is 0. Global cell index =
+// member << cshift | local index; `cells` and `spec` count the whole batch.
 struct Mesh {
     int R;
     int n;       // cells per side
     int shift;   // log2(n)
     size_t cells;
     int nh;      // n/2 + 1
-    size_t spec; // nh * n^(R-1)
+    size_t spec; // batch * nh * n^(R-1)
+    int cshift;  // R * shift: log2 of the cells of one member
+    size_t mspec;  // nh * n^(R-1): spectrum values of one member
+    int batch;
 };
 
-inline Mesh make_mesh(int R, int n) {
+inline Mesh make_mesh(int R, int n, int batch = 1) {
     Mesh m;
     m.R = R;
     m.n = n;
     m.shift = ilog2(n);
-    m.cells = 1;
-    for (int i = 0; i < R; ++i) m.cells *= (size_t)n;
+    m.cshift = R * m.shift;
+    m.batch = batch;
+    m.cells = (size_t)batch << m.cshift;
     m.nh = n / 2 + 1;
-    m.spec = (size_t)m.nh;
-    for (int i = 1; i < R; ++i) m.spec *= (size_t)n;
+    m.mspec = (size_t)m.nh;
+    for (int i = 1; i < R; ++i) m.mspec *= (size_t)n;
+    m.spec = m.mspec * (size_t)batch;
     return m;
 }
+
+// First global cell of the member owning global cell / spectrum element.
+__host__ __device__ inline size_t member_cells(const Mesh &m, size_t member) { return member << m.cshift; }
 
 // Signed integer wave number of index i on an n-mesh; index n/2 keeps the
 // positive sign like Fourier::kspace (src/base/fourier.hh:42-55).
 __host__ __device__ inline int wave_index(int i, int n) { return i > n / 2 ? i - n : i; }
 
-// Squared integer wave-vector length of half-spectrum element e.
+// Squared integer wave-vector length of half-spectrum element e (of any
+// member of the batch).
 __device__ inline long long spec_k2(size_t e, const Mesh &m, int *kv) {
+    if (m.batch > 1) e %= m.mspec;
     int kx = (int)(e % (size_t)m.nh);
     size_t rest = e / (size_t)m.nh;
     long long s = (long long)kx * kx;

@@ -18,7 +18,7 @@ struct FFTPair {
         dbl = is_double;
         int n[3];
         for (int i = 0; i < m.R; ++i) n[i] = m.n;  // cubic: slowest..fastest all n
-        long long real_dist = (long long)m.cells, cplx_dist = (long long)m.spec;
+        long long real_dist = 1LL << m.cshift, cplx_dist = (long long)m.mspec;
         size_t w1 = 0, w2 = 0;
         CONAN_CUFFT(cufftCreate(&r2c));
         CONAN_CUFFT(cufftCreate(&c2r));

@@ -248,6 +248,119 @@ template int potential_device<float>(const Mesh &, double, float *, cufftComplex
 template int potential_device<double>(const Mesh &, double, double *, cufftDoubleComplex *, FFTPair &,
                                       cudaStream_t);
 
+// out = in * f(k)^power * scale, DC = 0 (f the scale-free or CDM filter).
+template <typename T>
+__global__ void k_ic_filter_to(const typename Cplx<T>::type *__restrict__ in, typename Cplx<T>::type *__restrict__ out,
+                               Mesh m, ICFilter F, bool with_s, int power, double scale) {
+    size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.spec) return;
+    double f = 0.0;
+    if (e != 0) {
+        double v = ic_filter_value(F, m, e, with_s);
+        f = (power == 2 ? v * v : v) * scale;
+    }
+    auto z = in[e];
+    typename Cplx<T>::type r;
+    r.x = (T)((double)z.x * f);
+    r.y = (T)((double)z.y * f);
+    out[e] = r;
+}
+
+// Per-block sums of a . b (FP64, fixed order).
+template <typename T>
+__global__ void k_dot_partial(const T *__restrict__ a, const T *__restrict__ b, size_t n, double *__restrict__ part) {
+    double s = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        s += (double)a[i] * (double)b[i];
+    s = block_sum<double>(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// y += alpha x
+template <typename T> __global__ void k_axpy(T *__restrict__ y, const T *__restrict__ x, size_t n, double alpha) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = (T)((double)y[i] + alpha * (double)x[i]);
+}
+
+static ICFilter filter_of(const conan_ic_params &p, const Mesh &m) {
+    ICFilter F{};
+    F.mode = p.scale_free ? IC_SCALE_FREE : IC_CDM;
+    F.ns = p.ns;
+    F.L = p.size;
+    F.Omega0 = p.Omega0;
+    F.h = p.H0 / 100.0;
+    F.t = p.scale * m.n / p.size;
+    return F;
+}
+
+template <typename T> static int host_sum(const double *part, int nb, cudaStream_t st, double *out) {
+    std::vector<double> h(nb);
+    CONAN_CUDA(cudaMemcpyAsync(h.data(), part, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CONAN_CUDA(cudaStreamSynchronize(st));
+    double acc = 0;
+    for (int b = 0; b < nb; ++b) acc += h[b];
+    *out = acc;
+    return CONAN_OK;
+}
+
+// Adjoint of the Gaussian random field of grf_device: given the noise w and
+// dL/d(density) in dbar (overwritten), writes dL/dw into wbar. Scale-free:
+// density = s y with y = L_F w, s = sigma / sqrt(var), var = |L_PS w|^2 / N,
+// L_X = C2R diag(X) R2C / N (DC = 0), all symmetric, so
+//   wbar = s L_F dbar - (s / var) (y . dbar) / N  L_PS L_PS w.
+// CDM: density = A w with A symmetric, wbar = A dbar.
+// Scratch: spec, spec2 (half spectra), tmp (mesh); part >= 512 doubles.
+template <typename T>
+int grf_adjoint_device(const conan_ic_params &p, const Mesh &m, const T *w, T *dbar, T *wbar,
+                       typename Cplx<T>::type *spec, typename Cplx<T>::type *spec2, T *tmp, FFTPair &fft,
+                       double *part, cudaStream_t st) {
+    const ICFilter F = filter_of(p, m);
+    const unsigned gs = (unsigned)((m.spec + 255) / 256), gc = (unsigned)((m.cells + 255) / 256);
+    const double nc = (double)m.cells;
+    if (!p.scale_free) {
+        double scale = 1.0 / (nc * std::pow(p.size / m.n, 0.5 * m.R));
+        CONAN_TRY(fft.forward(dbar, spec));
+        k_ic_filter_to<T><<<gs, 256, 0, st>>>(spec, spec, m, F, false, 1, scale);
+        CONAN_LAUNCHED();
+        CONAN_TRY(fft.inverse(spec, wbar));
+        return CONAN_OK;
+    }
+    // W = R2C(w) (fft.forward leaves w intact for out-of-place R2C; copy to be safe)
+    CONAN_CUDA(cudaMemcpyAsync(tmp, w, m.cells * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    CONAN_TRY(fft.forward(tmp, spec));
+    const int nb = 512;
+    k_ic_var<T><<<nb, 256, 0, st>>>(spec, m, F, part);
+    CONAN_LAUNCHED();
+    double acc;
+    CONAN_TRY(host_sum<T>(part, nb, st, &acc));
+    const double var = acc / (nc * nc), s = p.sigma / std::sqrt(var);
+    // y = L_F w
+    k_ic_filter_to<T><<<gs, 256, 0, st>>>(spec, spec2, m, F, p.smooth != 0, 1, 1.0 / nc);
+    CONAN_LAUNCHED();
+    CONAN_TRY(fft.inverse(spec2, tmp));
+    k_dot_partial<T><<<nb, 256, 0, st>>>(tmp, dbar, m.cells, part);
+    CONAN_LAUNCHED();
+    double dot;
+    CONAN_TRY(host_sum<T>(part, nb, st, &dot));
+    // q = L_PS L_PS w into tmp
+    k_ic_filter_to<T><<<gs, 256, 0, st>>>(spec, spec2, m, F, true, 2, 1.0 / nc);
+    CONAN_LAUNCHED();
+    CONAN_TRY(fft.inverse(spec2, tmp));
+    // wbar = s L_F dbar
+    CONAN_TRY(fft.forward(dbar, spec));
+    k_ic_filter_to<T><<<gs, 256, 0, st>>>(spec, spec, m, F, p.smooth != 0, 1, s / nc);
+    CONAN_LAUNCHED();
+    CONAN_TRY(fft.inverse(spec, wbar));
+    k_axpy<T><<<gc, 256, 0, st>>>(wbar, tmp, m.cells, -(s / var) * dot / nc);
+    CONAN_LAUNCHED();
+    return CONAN_OK;
+}
+template int grf_adjoint_device<float>(const conan_ic_params &, const Mesh &, const float *, float *, float *,
+                                       cufftComplex *, cufftComplex *, float *, FFTPair &, double *, cudaStream_t);
+template int grf_adjoint_device<double>(const conan_ic_params &, const Mesh &, const double *, double *,
+                                        double *, cufftDoubleComplex *, cufftDoubleComplex *, double *, FFTPair &,
+                                        double *, cudaStream_t);
+
 template <typename T> int noise_device(const Mesh &m, unsigned long long seed, T *mesh, cudaStream_t st) {
     size_t pairs = (m.cells + 1) / 2;
     k_noise_philox<T><<<(unsigned)((pairs + 255) / 256), 256, 0, st>>>(mesh, m.cells, seed);

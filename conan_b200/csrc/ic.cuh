@@ -26,7 +26,13 @@ template <typename T> int noise_device(const Mesh &m, unsigned long long seed, T
 template <typename T>
 int grf_device(const conan_ic_params &p, const Mesh &m, T *mesh, typename Cplx<T>::type *spec, FFTPair &fft,
                double *part, cudaStream_t st);
-// Density mesh -> potential mesh, in place.
+// Adjoint of grf_device: dL/dw from dL/d(density) (dbar is overwritten).
+template <typename T>
+int grf_adjoint_device(const conan_ic_params &p, const Mesh &m, const T *w, T *dbar, T *wbar,
+                       typename Cplx<T>::type *spec, typename Cplx<T>::type *spec2, T *tmp, FFTPair &fft,
+                       double *part, cudaStream_t st);
+// Density mesh -> potential mesh, in place (a symmetric operator: it is its
+// own adjoint).
 template <typename T>
 int potential_device(const Mesh &m, double L, T *mesh, typename Cplx<T>::type *spec, FFTPair &fft,
                      cudaStream_t st);

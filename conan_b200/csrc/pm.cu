@@ -7,7 +7,10 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "ic.cuh"
 #include "pm.cuh"
+
+#include <type_traits>
 
 namespace conan {
 
@@ -117,11 +120,12 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
-    int create(const conan_pm_params &p) {
+    // `batch` equal boxes stored back to back (ensembles); 1 for conan_pm.
+    int create(const conan_pm_params &p, int batch = 1) {
         prm = p;
         int nf = p.n_mass * p.f;
-        mf = make_mesh(R, nf);
-        mm = make_mesh(R, p.n_mass);
+        mf = make_mesh(R, nf, batch);
+        mm = make_mesh(R, p.n_mass, batch);
         np = mm.cells;
         res_f = p.size / nf;
         res_m = p.size / p.n_mass;
@@ -131,6 +135,7 @@ template <typename T, int R> struct PM : PMBase {
         P.np = np;
         P.mshift = mm.shift;
         P.f = p.f;
+        P.bshift = R * mm.shift;
         for (int k = 0; k < R; ++k) {
             CONAN_TRY(alloc(&P.d[k], np));
             CONAN_TRY(alloc(&P.p[k], np));
@@ -152,7 +157,7 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TRY(alloc(&err, 1));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
         CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
-        CONAN_TRY(fft.create(mf, sizeof(T) == 8, 1));
+        CONAN_TRY(fft.create(mf, sizeof(T) == 8, batch));
         CONAN_TRY(alloc((char **)&work, fft.work_bytes));
         CONAN_TRY(fft.bind(work, st));
         CONAN_CUDA(cudaStreamSynchronize(st));
@@ -180,6 +185,24 @@ template <typename T, int R> struct PM : PMBase {
     dim3 grid_p() const { return dim3((unsigned)((np + 255) / 256)); }
 
     // --- deposit ---------------------------------------------------------
+    int dep_variant = 0;  // tile shape and block size (DepTile<R, V>), chosen by the autotuner
+
+    // Tiled deposit with tile variant V; returns 1 when V does not fit the
+    // mesh (the caller falls back), CONAN_OK or an error code.
+    template <int V> int deposit_tiles(double scale) {
+        typedef DepTile<R, V> D;
+        if (mf.n < D::TX || mf.n < D::TY || mf.n < D::TZ) return 1;
+        size_t tiles = (size_t)(mf.n / D::TX) * (R >= 2 ? mf.n / D::TY : 1) * (R == 3 ? mf.n / D::TZ : 1) *
+                       (size_t)mf.batch;
+        constexpr size_t sh = deposit_smem<T, R, V>();
+        auto kern = k_deposit<T, R, D::TX, D::TY, D::TZ, D::THREADS>;
+        if (sh > 48 * 1024)
+            CONAN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+        CONAN_TIMED(prof, "deposit", st,
+                    (kern<<<(unsigned)tiles, D::THREADS, sh, st>>>(off, pay, mesh, mf, scale, (uint32_t)np, err)));
+        return CONAN_OK;
+    }
+
     int rank_pass() {
         if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
         CONAN_TIMED(prof, "rank", st, (k_rank<T, R><<<grid_p(), 256, 0, st>>>(P, mf, count, rank)));
@@ -199,16 +222,12 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TIMED(prof, "scatter", st,
                     (k_scatter<T, R><<<grid_p(), 256, 0, st>>>(P, mf, off, rank, pay, nullptr)));
         double scale = mass;
-        typedef DepTile<R> D;
-        if (mf.n >= D::TX && mf.n >= D::TY && mf.n >= D::TZ) {
-            size_t tiles = (size_t)(mf.n / D::TX) * (R >= 2 ? mf.n / D::TY : 1) * (R == 3 ? mf.n / D::TZ : 1);
-            constexpr size_t sh = deposit_smem<T, R>();
-            auto kern = k_deposit<T, R, D::TX, D::TY, D::TZ, D::THREADS>;
-            if (sh > 48 * 1024)
-                CONAN_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-            CONAN_TIMED(prof, "deposit", st,
-                        (kern<<<(unsigned)tiles, D::THREADS, sh, st>>>(off, pay, mesh, mf, scale, (uint32_t)np, err)));
-        } else {
+        int rc = 1;  // 1: the variant does not fit this mesh
+        if (dep_variant == 1) rc = deposit_tiles<1>(scale);
+        if (dep_variant == 2) rc = deposit_tiles<2>(scale);
+        if (rc == 1) rc = deposit_tiles<0>(scale);
+        if (rc > 1) return rc;
+        if (rc == 1) {
             CONAN_TIMED(prof, "deposit", st,
                         (k_deposit_pull<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(
                             off, pay, mesh, mf, scale)));
@@ -516,6 +535,13 @@ template int spectrum_bins<float>(const cufftComplex *, const Mesh &, double, in
 template int spectrum_bins<double>(const cufftDoubleComplex *, const Mesh &, double, int, double *,
                                    double *, double *, cudaStream_t, PMBase *);
 
+}  // namespace conan
+
+#include "adjoint_impl.cuh"
+#include "ensemble_impl.cuh"
+
+namespace conan {
+
 PMBase *make_pm(const conan_pm_params &p) {
     PMBase *b = nullptr;
     int rc = CONAN_OK;
@@ -661,6 +687,151 @@ int conan_pm_get_stream(conan_pm *h, void **stream) {
     if (!stream) return set_error(CONAN_ERR_ARG, "null pointer");
     *stream = h->impl->stream();
     return CONAN_OK;
+}
+
+}  // extern "C"
+
+struct conan_diff {
+    DiffBase *impl;
+};
+
+extern "C" {
+
+conan_diff *conan_diff_create(const conan_diff_params *p) {
+    last_error().clear();
+    if (!p) {
+        set_error(CONAN_ERR_ARG, "null parameters");
+        return nullptr;
+    }
+    if (check_pm_params(&p->pm) != CONAN_OK || check_ic_params(&p->ic) != CONAN_OK) return nullptr;
+    if (p->ic.dim != p->pm.dim || (1 << p->ic.mbits) != p->pm.n_mass) {
+        set_error(CONAN_ERR_ARG, "ic and pm parameters disagree on dim / particles per side");
+        return nullptr;
+    }
+    if (p->pm.gradient != CONAN_GRAD_FD4) {
+        set_error(CONAN_ERR_UNSUPPORTED, "the adjoint supports the FD4 gradient only");
+        return nullptr;
+    }
+    if (p->n < 1 || !(p->da > 0) || !(p->a0 > 0)) {
+        set_error(CONAN_ERR_ARG, "need n >= 1, a0 > 0, da > 0");
+        return nullptr;
+    }
+    if (device_guard(p->pm.device) != CONAN_OK) return nullptr;
+    DiffBase *b = make_diff(*p);
+    if (!b) return nullptr;
+    return new conan_diff{b};
+}
+
+void conan_diff_destroy(conan_diff *h) {
+    if (!h) return;
+    if (h->impl) {
+        cudaSetDevice(h->impl->device());
+        delete h->impl;
+    }
+    delete h;
+}
+
+int conan_diff_forward(conan_diff *h, const void *noise_dev, void *density_out_dev, void *stream) {
+    if (!h || !h->impl) return set_error(CONAN_ERR_ARG, "null handle");
+    if (!noise_dev || !density_out_dev) return set_error(CONAN_ERR_ARG, "null buffer");
+    CONAN_TRY(device_guard(h->impl->device()));
+    return h->impl->forward(noise_dev, density_out_dev, stream);
+}
+
+int conan_diff_backward(conan_diff *h, const void *grad_density_dev, void *grad_noise_dev, void *stream) {
+    if (!h || !h->impl) return set_error(CONAN_ERR_ARG, "null handle");
+    if (!grad_density_dev || !grad_noise_dev) return set_error(CONAN_ERR_ARG, "null buffer");
+    CONAN_TRY(device_guard(h->impl->device()));
+    return h->impl->backward(grad_density_dev, grad_noise_dev, stream);
+}
+
+}  // extern "C"
+
+struct conan_ens {
+    EnsBase *impl;
+};
+
+#define ENS_GUARD(h)                                                              \
+    do {                                                                          \
+        if (!(h) || !(h)->impl) return set_error(CONAN_ERR_ARG, "null handle");   \
+        CONAN_TRY(device_guard((h)->impl->device()));                             \
+    } while (0)
+
+extern "C" {
+
+conan_ens *conan_ens_create(const conan_ens_params *p, int n_members, const conan_ens_member *m) {
+    last_error().clear();
+    if (!p || !m || n_members < 1) {
+        set_error(CONAN_ERR_ARG, "need parameters and at least one member");
+        return nullptr;
+    }
+    if (p->dim != 2 && p->dim != 3) {
+        set_error(CONAN_ERR_UNSUPPORTED, "ensembles run in 2 or 3 dimensions");
+        return nullptr;
+    }
+    if (p->n < 1 || !(p->a0 > 0) || !(p->da > 0) || !(p->H0 > 0) ||
+        (p->precision != CONAN_FP32 && p->precision != CONAN_FP64)) {
+        set_error(CONAN_ERR_ARG, "bad run parameters (n >= 1, a0, da, H0 > 0, precision)");
+        return nullptr;
+    }
+    for (int i = 0; i < n_members; ++i)
+        if (m[i].mbits < 3 || m[i].mbits > (p->dim == 3 ? 10 : 14) || !(m[i].size > 0)) {
+            set_error(CONAN_ERR_ARG, "member %d: mbits %d / size %g out of range", i, m[i].mbits, m[i].size);
+            return nullptr;
+        }
+    if (device_guard(p->device) != CONAN_OK) return nullptr;
+    EnsBase *b = make_ens(*p, n_members, m);
+    if (!b) return nullptr;
+    return new conan_ens{b};
+}
+
+void conan_ens_destroy(conan_ens *h) {
+    if (!h) return;
+    if (h->impl) {
+        cudaSetDevice(h->impl->device());
+        delete h->impl;
+    }
+    delete h;
+}
+
+int conan_ens_init(conan_ens *h) {
+    ENS_GUARD(h);
+    return h->impl->init();
+}
+int conan_ens_run(conan_ens *h) {
+    ENS_GUARD(h);
+    return h->impl->run();
+}
+int conan_ens_forward_adjoint(conan_ens *h, double *loss_out) {
+    ENS_GUARD(h);
+    return h->impl->forward_adjoint(loss_out);
+}
+int conan_ens_power_spectrum(conan_ens *h, int member, int nbins, double *k, double *P, double *count) {
+    ENS_GUARD(h);
+    if (nbins < 1) return set_error(CONAN_ERR_ARG, "nbins must be positive");
+    return h->impl->power_spectrum(member, nbins, k, P, count);
+}
+int conan_ens_state(conan_ens *h, int member, double *X, double *P) {
+    ENS_GUARD(h);
+    return h->impl->state(member, X, P);
+}
+int conan_ens_last_ms(conan_ens *h, double *run_ms, double *adjoint_ms) {
+    ENS_GUARD(h);
+    return h->impl->last_ms(run_ms, adjoint_ms);
+}
+int conan_ens_total_particles(conan_ens *h, size_t *n) {
+    ENS_GUARD(h);
+    if (!n) return set_error(CONAN_ERR_ARG, "null pointer");
+    *n = h->impl->total_particles();
+    return CONAN_OK;
+}
+int conan_ens_describe(conan_ens *h, char *buf, size_t len) {
+    ENS_GUARD(h);
+    if (!buf || len == 0) return set_error(CONAN_ERR_ARG, "null buffer");
+    std::string s = h->impl->describe();
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = 0;
+    return s.size() < len ? CONAN_OK : set_error(CONAN_ERR_ARG, "buffer too small (%zu bytes needed)", s.size() + 1);
 }
 
 }  // extern "C"

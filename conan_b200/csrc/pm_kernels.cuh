@@ -9,18 +9,21 @@
 // P = p * res_f (src/run/nbody.hh:46-50,88-95).
 //
 // Deposit (md_cic, src/run/numeric.hh:106-139) runs as a counting sort by
-// cell id followed by a warp-segmented reduction:
+// cell id followed by a tiled shared-memory reduction:
 //   rank   : cell id of every particle (integer, periodic wrap), rank within
 //            its cell from an integer counter (fused into the drift),
 //   scan   : exclusive prefix of the per-cell counts -> cell offsets,
 //   scatter: the particle's cell fractions written at offset + rank,
-//   reduce : each warp walks a 32-cell row of cells in sorted order; the
-//            2^R corner weights of each particle are quantised to integers
-//            and summed per cell with redux.sync over runs of lanes holding
-//            the same cell, then combined with the neighbouring rows and
-//            planes in registers. All sums are integer, so the density is
-//            bit-identical from run to run whatever order the sort produced
-//            inside a cell; no floating-point atomics are used.
+//   reduce : one CTA per output tile stages the tile's cell offsets in
+//            shared memory and walks the sorted particles of its source
+//            cells in equal slices; the 2^R corner weights of each particle
+//            are quantised to integers, summed per cell in registers and
+//            flushed into integer tile accumulators. All sums are integer, so
+//            the density is bit-identical from run to run whatever order the
+//            sort produced inside a cell; no floating-point atomics are used.
+// Every kernel also handles a batch of equal boxes stored back to back
+// (ensembles): the member index sits in the high bits of particle and cell
+// indices.
 #pragma once
 
 #include "common.cuh"
@@ -29,13 +32,22 @@ namespace conan {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Particles of a batch of boxes: particle i belongs to member i >> bshift
+// and sits at lattice point i & ((1 << bshift) - 1) of that member.
 template <typename T> struct Parts {
     T *d[3];
     T *p[3];
-    size_t np;
+    size_t np;   // whole batch
     int mshift;  // log2(N_m)
     int f;       // force cells per lattice spacing
+    int bshift;  // R * mshift
 };
+
+// First global force-mesh cell of particle i's member.
+template <typename T>
+__host__ __device__ inline size_t cell_base(const Parts<T> &P, const Mesh &m, size_t i) {
+    return (i >> P.bshift) << m.cshift;
+}
 
 template <typename T, int R>
 __device__ inline void lattice(const Parts<T> &P, size_t i, int *q) {
@@ -138,7 +150,7 @@ __global__ void __launch_bounds__(256) k_rank(Parts<T> P, Mesh m, uint32_t *__re
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.np) return;
     uint32_t c = deposit_cell<T, R>(P, m, i);
-    rank[i] = atomicAdd(count + c, 1u);
+    rank[i] = atomicAdd(count + cell_base(P, m, i) + c, 1u);
 }
 
 // ------------------------------------------------------------ scan --
@@ -280,7 +292,7 @@ __global__ void __launch_bounds__(256) k_scatter(Parts<T> P, Mesh m, const uint3
             c = (c << m.shift) | (uint32_t)ck;
             word |= (unsigned long long)fr << (21 * k);
         }
-        uint32_t dst = off[c] + rank[i];
+        uint32_t dst = off[cell_base(P, m, i) + c] + rank[i];
         if (dst >= P.np) return;  // unreachable when counts and ranks agree
         pay[dst] = word;
         if (sorted_idx) sorted_idx[dst] = (uint32_t)i;
@@ -292,7 +304,7 @@ __global__ void __launch_bounds__(256) k_scatter(Parts<T> P, Mesh m, const uint3
             Pay<double>::cell_frac(P.d[k][i], q[k], m.n - 1, &ck, &fr[k]);
             c = (c << m.shift) | (uint32_t)ck;
         }
-        uint32_t dst = off[c] + rank[i];
+        uint32_t dst = off[cell_base(P, m, i) + c] + rank[i];
         if (dst >= P.np) return;  // unreachable when counts and ranks agree
 #pragma unroll
         for (int k = 0; k < R; ++k) pay[(size_t)dst * R + k] = fr[k];
@@ -375,10 +387,19 @@ __device__ inline unsigned long long quant_w(double w) {
 }
 
 // Tile shape of the deposit for dimension R: TX x TY x TZ output cells.
-template <int R> struct DepTile;
-template <> struct DepTile<3> { static constexpr int TX = 32, TY = 8, TZ = 8, THREADS = 256; };
-template <> struct DepTile<2> { static constexpr int TX = 32, TY = 32, TZ = 1, THREADS = 256; };
-template <> struct DepTile<1> { static constexpr int TX = 1024, TY = 1, TZ = 1, THREADS = 256; };
+// Variant V (0 = default) of the tile shape; the autotuner picks one per
+// mesh size.
+constexpr int DEP_VARIANTS = 3;
+template <int R, int V = 0> struct DepTile;
+template <> struct DepTile<3, 0> { static constexpr int TX = 32, TY = 8, TZ = 8, THREADS = 256; };
+template <> struct DepTile<3, 1> { static constexpr int TX = 32, TY = 4, TZ = 8, THREADS = 128; };
+template <> struct DepTile<3, 2> { static constexpr int TX = 32, TY = 16, TZ = 8, THREADS = 512; };
+template <> struct DepTile<2, 0> { static constexpr int TX = 32, TY = 32, TZ = 1, THREADS = 256; };
+template <> struct DepTile<2, 1> { static constexpr int TX = 32, TY = 16, TZ = 1, THREADS = 128; };
+template <> struct DepTile<2, 2> { static constexpr int TX = 64, TY = 32, TZ = 1, THREADS = 512; };
+template <> struct DepTile<1, 0> { static constexpr int TX = 1024, TY = 1, TZ = 1, THREADS = 256; };
+template <> struct DepTile<1, 1> { static constexpr int TX = 512, TY = 1, TZ = 1, THREADS = 128; };
+template <> struct DepTile<1, 2> { static constexpr int TX = 2048, TY = 1, TZ = 1, THREADS = 512; };
 
 // One CTA deposits one output tile. Its source cells are the tile plus one
 // cell on the low side of every axis (a particle in cell s reaches s..s+1).
@@ -390,7 +411,7 @@ template <> struct DepTile<1> { static constexpr int TX = 1024, TY = 1, TZ = 1, 
 // tile's integer accumulators when the cell changes. Integer sums make the
 // result independent of the order of particles and flushes.
 template <typename T, int R, int TX, int TY, int TZ, int THREADS>
-__global__ void __launch_bounds__(THREADS, 4)
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     k_deposit(const uint32_t *__restrict__ off, const typename Pay<T>::elem *__restrict__ pay,
               T *__restrict__ out, Mesh m, double scale, uint32_t np, int *__restrict__ err) {
     constexpr int HY = R >= 2 ? 1 : 0, HZ = R == 3 ? 1 : 0;
@@ -404,8 +425,12 @@ __global__ void __launch_bounds__(THREADS, 4)
     uint32_t *rp = raw + NR * RAW;  // NR + 1 row prefixes
 
     const int n = m.n, mask = n - 1;
-    const int ntx = n / TX, nty = R >= 2 ? n / TY : 1;
-    const int tile = blockIdx.x;
+    const int ntx = n / TX, nty = R >= 2 ? n / TY : 1, ntz = R == 3 ? n / TZ : 1;
+    const int tiles = ntx * nty * ntz;  // per member of the batch
+    const size_t mbase = member_cells(m, blockIdx.x / tiles);
+    off += mbase;
+    out += mbase;
+    const int tile = blockIdx.x % tiles;
     const int x0 = (tile % ntx) * TX;
     const int y0 = R >= 2 ? ((tile / ntx) % nty) * TY : 0;
     const int z0 = R == 3 ? (tile / (ntx * nty)) * TZ : 0;
@@ -555,8 +580,8 @@ __global__ void __launch_bounds__(THREADS, 4)
     }
 }
 
-template <typename T, int R> constexpr size_t deposit_smem() {
-    typedef DepTile<R> D;
+template <typename T, int R, int V = 0> constexpr size_t deposit_smem() {
+    typedef DepTile<R, V> D;
     constexpr int HY = R >= 2 ? 1 : 0, HZ = R == 3 ? 1 : 0;
     constexpr int NR = (D::TY + HY) * (D::TZ + HZ);
     return sizeof(uint32_t) * (Slot<T>::W * D::TX * D::TY * D::TZ + NR * (D::TX + 3) + NR + 1);
@@ -580,6 +605,7 @@ __global__ void k_deposit_pull(const uint32_t *__restrict__ off,
         size_t sc = 0;
         for (int k = R - 1; k >= 0; --k)
             sc = (sc << m.shift) | (size_t)((x[k] - ((b >> k) & 1)) & (m.n - 1));
+        sc += member_cells(m, c >> m.cshift);
         for (uint32_t j = off[sc]; j < off[sc + 1]; ++j) {
             T fr[3];
             load_frac<T, R>(pay, j, fr);
@@ -707,6 +733,7 @@ __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, 
         F[k] = T(0);
     }
     const int mask = m.n - 1;
+    const size_t cb = cell_base(P, m, i);
     if constexpr (SPECTRAL) {
 #pragma unroll
         for (int b = 0; b < (1 << R); ++b) {
@@ -717,7 +744,7 @@ __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, 
 #pragma unroll
             for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
 #pragma unroll
-            for (int k = 0; k < R; ++k) F[k] += __ldg(g[k] + ci) * z;
+            for (int k = 0; k < R; ++k) F[k] += __ldg(g[k] + cb + ci) * z;
         }
     } else {
         // FD4 gradient of the corner nodes from the packed gradient mesh
@@ -731,7 +758,7 @@ __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, 
             T z = 1;
 #pragma unroll
             for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
-            G4<T> gv = load_g4(G + ci);
+            G4<T> gv = load_g4(G + cb + ci);
             F[0] += gv.x * z;
             if (R > 1) F[1] += gv.y * z;
             if (R > 2) F[2] += gv.z * z;
@@ -800,7 +827,7 @@ __global__ void __launch_bounds__(256)
             P.d[k][i] = d[k];
         }
     }
-    if (c.rank) rank[i] = atomicAdd(count + deposit_cell<T, R>(P, m, i), 1u);
+    if (c.rank) rank[i] = atomicAdd(count + cell_base(P, m, i) + deposit_cell<T, R>(P, m, i), 1u);
 }
 
 // ------------------------------------------------------------ init/io --
@@ -817,7 +844,7 @@ __global__ void k_zeldovich(Parts<T> P, const T *__restrict__ phim, Mesh mm, dou
     for (int k = 0; k < R; ++k) c[k] = (int)((i >> (k * mm.shift)) & (size_t)(mm.n - 1));
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        T u = fd4<T, R>(phim, c, k, mm.shift, mm.n - 1);
+        T u = fd4<T, R>(phim + member_cells(mm, i >> P.bshift), c, k, mm.shift, mm.n - 1);
         P.d[k][i] = u * (T)cdz;
         P.p[k][i] = u * (T)cpz;
     }

@@ -255,6 +255,8 @@ int conan_ens_state(conan_ens *h, int member, double *X, double *P);
 /* Milliseconds of the last conan_ens_run / forward_adjoint (CUDA events). */
 int conan_ens_last_ms(conan_ens *h, double *run_ms, double *adjoint_ms);
 int conan_ens_total_particles(conan_ens *h, size_t *n);
+/* JSON description of the size classes and the autotuner's choices. */
+int conan_ens_describe(conan_ens *h, char *buf, size_t len);
 
 #ifdef __cplusplus
 }

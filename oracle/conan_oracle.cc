@@ -443,3 +443,243 @@ void oracle_power_spectrum(int R, int N, double L, const double *delta, int nbin
 }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------------
+ * FP64 CPU adjoint of the differentiable model (no reference counterpart:
+ * the reference has no adjoint). Forward: white noise w -> scale-free GRF
+ * (oracle_grf_scale_free) -> potential (oracle_potential) -> Zel'dovich
+ * (oracle_zeldovich) -> n leapfrog steps (oracle_drift / oracle_kick) ->
+ * final CIC density (oracle_md_cic - 1). The adjoint is derived directly in
+ * the reference's physical units (absolute X, momentum P), keeping every
+ * forward state in memory (small test sizes only).
+ * ---------------------------------------------------------------------- */
+namespace {
+
+struct DiffCfg {
+    int R, mbits, f;
+    double L, ns, scale, sigma, H0, Om, OL, a0, da;
+    int smooth;
+    unsigned n;
+};
+
+/* Linear Fourier operator on an R-cube: out = Re IFFT(FFT(in) * mult) / size,
+ * mult(idx) given, DC forced to zero. */
+template <typename M>
+void fourier_op(int R, int N, const double *in, double *out, M mult) {
+    size_t size = ipow(N, R);
+    std::vector<cplx> a(size), b(size);
+    for (size_t i = 0; i < size; ++i) a[i] = in[i];
+    dft(a, b, R, N, FFTW_FORWARD);
+    for (size_t i = 0; i < size; ++i) a[i] = b[i] * mult(i);
+    a[0] = 0;
+    dft(a, b, R, N, FFTW_BACKWARD);
+    for (size_t i = 0; i < size; ++i) out[i] = b[i].real() / (double)size;
+}
+
+/* dW_b/dx_k for CIC weights with A0 = 1 - A1. */
+double dW(const double *A0, const double *A1, int R, int b, int k) {
+    double z = ((b >> k) & 1) ? 1.0 : -1.0;
+    for (int l = 0; l < R; ++l)
+        if (l != k) z *= ((b >> l) & 1) ? A1[l] : A0[l];
+    return z;
+}
+
+/* -sum_k FD4_k(U_k) / res on an R-cube (the adjoint of the FD4 gradient). */
+void neg_div(int R, int N, double res, const std::vector<std::vector<double>> &U, double *out) {
+    size_t size = ipow(N, R);
+    for (size_t x = 0; x < size; ++x) {
+        int p0[8], q[8];
+        decode(x, R, N, p0);
+        double acc = 0;
+        for (int k = 0; k < R; ++k) {
+            size_t id[4];
+            int off[4] = {-2, -1, 1, 2};
+            for (int j = 0; j < 4; ++j) {
+                std::memcpy(q, p0, sizeof(int) * R);
+                q[k] += off[j];
+                id[j] = box_idx(q, R, N);
+            }
+            const std::vector<double> &u = U[k];
+            acc += u[id[0]] / 12. - 2 * u[id[1]] / 3. + 2 * u[id[2]] / 3. - u[id[3]] / 12.;
+        }
+        out[x] = -acc / res;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+/* noisebar = dL/dw for L with dL/d(final density) = deltabar. Also writes
+ * the final density into delta_out (may be NULL). */
+void oracle_diff_adjoint(int R, int mbits, int f, double L, double ns, int smooth, double scale, double sigma,
+                         double H0, double Om, double OL, double a0, double da, unsigned n, const double *w,
+                         const double *deltabar, double *delta_out, double *noisebar) {
+    const int Nm = 1 << mbits, Nf = Nm * f;
+    const size_t np = ipow(Nm, R), nc = ipow(Nf, R);
+    const double res_f = L / Nf, res_m = L / Nm, mass = std::pow((double)Nf / Nm, R);
+    const double Gc = 3. / 2 * Om * H0 * H0;
+    /* ---- forward, keeping states ---- */
+    std::vector<double> dens(np), phim(np);
+    oracle_grf_scale_free(R, mbits, L, ns, smooth, scale, sigma, w, dens.data());
+    phim = dens;
+    oracle_potential(R, mbits, L, phim.data());
+    std::vector<double> X(np * R), P(np * R);
+    double a_pos = a0, a_mom = a0 + da / 2;
+    oracle_zeldovich(R, Nm, L, phim.data(), a_pos, a_mom, X.data(), P.data());
+    std::vector<std::vector<double>> Xs(n), phis(n);  // positions at the kicks and their potentials
+    std::vector<double> as(n);
+    double a = a0;
+    for (unsigned i = 0; i < n; ++i) {
+        as[i] = a;
+        oracle_drift(R, Nm, H0, Om, OL, X.data(), P.data(), a, da);
+        Xs[i] = X;
+        phis[i].resize(nc);
+        oracle_kick(R, Nm, f, L, H0, Om, OL, X.data(), P.data(), a + da / 2, da, phis[i].data());
+        a += da;
+    }
+    std::vector<double> dfin(nc);
+    oracle_md_cic(R, Nf, L, X.data(), np, mass, dfin.data());
+    if (delta_out)
+        for (size_t c = 0; c < nc; ++c) delta_out[c] = dfin[c] - 1.0;
+
+    /* deposit-weight frame of a particle: cells and weights of md_cic */
+    auto dep_frame = [&](const double *x, int *origin, double *A0, double *A1) {
+        for (int k = 0; k < R; ++k) {
+            double p0 = dmod(x[k], L) / res_f;
+            origin[k] = (int)p0;
+            A1[k] = p0 - origin[k];
+            A0[k] = 1 - A1[k];
+        }
+    };
+    auto gat_frame = [&](const double *x, int *origin, double *A0, double *A1) {
+        for (int k = 0; k < R; ++k) {
+            double xx = x[k] / res_f;
+            origin[k] = (int)xx;
+            A1[k] = xx - origin[k];
+            A0[k] = 1 - A1[k];
+        }
+    };
+    auto corner = [&](const int *origin, int b) {
+        int c[8];
+        for (int k = 0; k < R; ++k) c[k] = origin[k] + ((b >> k) & 1);
+        return box_idx(c, R, Nf);
+    };
+    auto poisson_op = [&](const double *in, double *out, double am) {
+        fourier_op(R, Nf, in, out, [&](size_t i) {
+            double k[8];
+            kvec(i, R, Nf, L, k);
+            return cplx(-1. / sqr(k, R) * Gc / am);
+        });
+    };
+
+    /* ---- backward ---- */
+    std::vector<double> Xb(np * R, 0.0), Pb(np * R, 0.0);
+    for (size_t j = 0; j < np; ++j) {  // through the final deposit
+        int o[8];
+        double A0[8], A1[8];
+        dep_frame(&X[j * R], o, A0, A1);
+        for (int b = 0; b < (1 << R); ++b) {
+            double v = deltabar[corner(o, b)];
+            for (int k = 0; k < R; ++k) Xb[j * R + k] += mass * dW(A0, A1, R, b, k) * v / res_f;
+        }
+    }
+    for (int i = (int)n - 1; i >= 0; --i) {
+        const double am = as[i] + da / 2;
+        const double ckp = da / oracle_adot(H0, Om, OL, am);
+        const double cdp = da / (as[i] * as[i] * oracle_adot(H0, Om, OL, as[i]));
+        const std::vector<double> &Xk = Xs[i];
+        const std::vector<double> &phi = phis[i];
+        std::vector<double> g(nc * R);
+        oracle_gradient(R, Nf, L, phi.data(), g.data());  // physical gradient at the nodes
+        const std::vector<double> v = Pb;
+        // U_k = gather-transpose deposit of v_k
+        std::vector<std::vector<double>> U(R, std::vector<double>(nc, 0.0));
+        for (size_t j = 0; j < np; ++j) {
+            int o[8];
+            double A0[8], A1[8];
+            gat_frame(&Xk[j * R], o, A0, A1);
+            for (int b = 0; b < (1 << R); ++b) {
+                double z = 1;
+                for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? A1[k] : A0[k];
+                size_t c = corner(o, b);
+                for (int k = 0; k < R; ++k) U[k][c] += v[j * R + k] * z;
+            }
+        }
+        std::vector<double> div(nc), rhob(nc);
+        neg_div(R, Nf, res_f, U, div.data());
+        poisson_op(div.data(), rhob.data(), am);
+        for (size_t j = 0; j < np; ++j) {
+            double t1[8] = {0}, t2[8] = {0};
+            int o[8];
+            double A0[8], A1[8];
+            gat_frame(&Xk[j * R], o, A0, A1);
+            for (int b = 0; b < (1 << R); ++b) {
+                size_t c = corner(o, b);
+                double vg = 0;
+                for (int k = 0; k < R; ++k) vg += v[j * R + k] * g[c * R + k];
+                for (int k = 0; k < R; ++k) t1[k] += dW(A0, A1, R, b, k) * vg / res_f;
+            }
+            dep_frame(&Xk[j * R], o, A0, A1);
+            for (int b = 0; b < (1 << R); ++b) {
+                double r = rhob[corner(o, b)];
+                for (int k = 0; k < R; ++k) t2[k] += mass * dW(A0, A1, R, b, k) * r / res_f;
+            }
+            for (int k = 0; k < R; ++k) {
+                double xb = Xb[j * R + k] - ckp * (t1[k] + t2[k]);
+                Xb[j * R + k] = xb;
+                Pb[j * R + k] = v[j * R + k] + cdp * xb;
+            }
+        }
+    }
+    /* Zel'dovich: X = q - a_pos u, P = -a_mom u, u = FD4(phi_m)/res_m */
+    std::vector<std::vector<double>> ub(R, std::vector<double>(np));
+    for (size_t j = 0; j < np; ++j)
+        for (int k = 0; k < R; ++k) ub[k][j] = -a_pos * Xb[j * R + k] - a_mom * Pb[j * R + k];
+    std::vector<double> phib(np), densb(np);
+    neg_div(R, Nm, res_m, ub, phib.data());
+    /* potential operator (symmetric): -1/k^2 physical, DC 0 */
+    fourier_op(R, Nm, phib.data(), densb.data(), [&](size_t i) {
+        double k[8];
+        kvec(i, R, Nm, L, k);
+        return cplx(-1. / sqr(k, R));
+    });
+    /* random field: dens = s y, y = L_F w, var = |L_PS w|^2 / N, s = sigma/sqrt(var) */
+    const double t = scale * Nm / L;
+    auto PSf = [&](size_t i, bool with_s) {
+        double k[8];
+        kvec(i, R, Nm, (double)Nm, k);
+        double p = std::sqrt(std::pow(std::sqrt(sqr(k, R)), ns));
+        return with_s ? p * scale_filter(k, R, t) : p;
+    };
+    std::vector<double> y(np), z(np), q(np), lfd(np);
+    fourier_op(R, Nm, w, y.data(), [&](size_t i) { return cplx(PSf(i, smooth != 0)); });
+    fourier_op(R, Nm, w, z.data(), [&](size_t i) { return cplx(PSf(i, true)); });
+    fourier_op(R, Nm, z.data(), q.data(), [&](size_t i) { return cplx(PSf(i, true)); });
+    fourier_op(R, Nm, densb.data(), lfd.data(), [&](size_t i) { return cplx(PSf(i, smooth != 0)); });
+    double var = 0, dot = 0;
+    for (size_t j = 0; j < np; ++j) {
+        var += z[j] * z[j];
+        dot += y[j] * densb[j];
+    }
+    var /= (double)np;
+    const double s = sigma / std::sqrt(var);
+    for (size_t j = 0; j < np; ++j) noisebar[j] = s * lfd[j] - (s / var) * dot / (double)np * q[j];
+}
+
+/* The forward model alone: final CIC density contrast from the noise. */
+void oracle_diff_forward(int R, int mbits, int f, double L, double ns, int smooth, double scale, double sigma,
+                         double H0, double Om, double OL, double a0, double da, unsigned n, const double *w,
+                         double *delta_out) {
+    const int Nm = 1 << mbits, Nf = Nm * f;
+    const size_t np = ipow(Nm, R), nc = ipow(Nf, R);
+    std::vector<double> dens(np);
+    oracle_grf_scale_free(R, mbits, L, ns, smooth, scale, sigma, w, dens.data());
+    oracle_potential(R, mbits, L, dens.data());
+    std::vector<double> X(np * R), P(np * R);
+    oracle_run(R, Nm, f, L, H0, Om, OL, dens.data(), a0, da, n, X.data(), P.data());
+    oracle_md_cic(R, Nf, L, X.data(), np, std::pow((double)Nf / Nm, R), delta_out);
+    for (size_t c = 0; c < nc; ++c) delta_out[c] -= 1.0;
+}
+
+}  // extern "C"

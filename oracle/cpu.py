@@ -135,3 +135,24 @@ def power_spectrum(dim, N, L, delta, nbins=None):
     k, p, c = np.empty(nb), np.empty(nb), np.empty(nb)
     lib().oracle_power_spectrum(dim, N, _d(L), P(delta), nb, P(k), P(p), P(c))
     return k, p, c
+
+
+def diff_forward(dim, mbits, f, L, ns, smooth, scale, sigma, a0, da, n, noise, H0=68.5, Om=1.0, OL=0.0):
+    """Final CIC density contrast of the differentiable model (FP64 CPU)."""
+    noise = np.ascontiguousarray(noise, dtype=np.float64)
+    out = np.empty(((1 << mbits) * f) ** dim)
+    lib().oracle_diff_forward(dim, mbits, f, _d(L), _d(ns), int(smooth), _d(scale), _d(sigma), _d(H0), _d(Om),
+                              _d(OL), _d(a0), _d(da), C.c_uint(n), P(noise), P(out))
+    return out
+
+
+def diff_adjoint(dim, mbits, f, L, ns, smooth, scale, sigma, a0, da, n, noise, deltabar, H0=68.5, Om=1.0,
+                 OL=0.0):
+    """(final density contrast, dL/dnoise) for dL/d(density) = deltabar (FP64 CPU adjoint)."""
+    noise = np.ascontiguousarray(noise, dtype=np.float64)
+    deltabar = np.ascontiguousarray(deltabar, dtype=np.float64)
+    dens = np.empty(deltabar.size)
+    gb = np.empty_like(noise)
+    lib().oracle_diff_adjoint(dim, mbits, f, _d(L), _d(ns), int(smooth), _d(scale), _d(sigma), _d(H0), _d(Om),
+                              _d(OL), _d(a0), _d(da), C.c_uint(n), P(noise), P(deltabar), P(dens), P(gb))
+    return dens, gb
