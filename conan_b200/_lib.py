@@ -14,6 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libconan_pm.so"
 OK, ERR_ARG, ERR_ALLOC, ERR_CUDA, ERR_TIMEOUT, ERR_IO, ERR_STATE, ERR_UNSUPPORTED = range(8)
 FP32, FP64 = 0, 1
 GRAD_FD4, GRAD_SPECTRAL = 0, 1
+DEPOSIT_SORTED, DEPOSIT_LAGRANGIAN = 0, 1
 
 _dp = C.POINTER(C.c_double)
 
@@ -64,6 +65,8 @@ SIGNATURES = {
     "conan_pm_drift": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     "conan_pm_kick": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
     "conan_pm_set_callback_interval": (C.c_int, [C.c_void_p, C.c_uint]),
+    "conan_pm_set_deposit": (C.c_int, [C.c_void_p, C.c_int]),
+    "conan_pm_get_deposit": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "conan_pm_run": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double, C.c_uint, STEP_CB, C.c_void_p]),
     "conan_pm_get_state": (C.c_int, [C.c_void_p, _dp, _dp]),
     "conan_pm_set_state": (C.c_int, [C.c_void_p, _dp, _dp, C.c_double, C.c_double]),

@@ -52,7 +52,7 @@ template <typename T, int R> struct Ens : EnsBase {
         T *noise = nullptr, *tnoise = nullptr, *target = nullptr, *dens = nullptr, *gd = nullptr, *gn = nullptr;
         T *s0[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
         cudaEvent_t join = nullptr, t0 = nullptr, t1 = nullptr;
-        double tune_ms[DEP_VARIANTS] = {0, 0, 0};
+        double tune_ms[DEP_VARIANTS + 1] = {0, 0, 0, 0};  // sorted tiles, then Lagrangian (-1: not run)
     };
     conan_ens_params prm{};
     std::vector<conan_ens_member> mem;
@@ -180,7 +180,9 @@ template <typename T, int R> struct Ens : EnsBase {
         auto &pm = c.d->pm;
         double best = 1e30;
         int bv = 0;
-        for (int v = 0; v < DEP_VARIANTS; ++v) {
+        c.tune_ms[DEP_VARIANTS] = -1;
+        const int nv = pm.lag_v >= 0 && pm.lacc ? DEP_VARIANTS + 1 : DEP_VARIANTS;
+        for (int v = 0; v < nv; ++v) {
             pm.dep_variant = v;
             CONAN_TRY(pm.deposit());
             CONAN_CUDA(cudaEventRecord(c.t0, pm.st));
@@ -358,9 +360,10 @@ template <typename T, int R> struct Ens : EnsBase {
             char buf[256];
             snprintf(buf, sizeof buf,
                      "%s{\"mesh\": %d, \"L\": %g, \"members\": %zu, \"deposit_variant\": %d, "
-                     "\"tune_ms\": [%.4f, %.4f, %.4f]}",
-                     i ? ", " : "", 1 << c.mbits, c.L, c.members.size(), c.d->pm.dep_variant, c.tune_ms[0],
-                     c.tune_ms[1], c.tune_ms[2]);
+                     "\"deposit\": \"%s\", \"tune_ms\": [%.4f, %.4f, %.4f, %.4f]}",
+                     i ? ", " : "", 1 << c.mbits, c.L, c.members.size(), c.d->pm.dep_variant,
+                     c.d->pm.lag_on() ? "lagrangian" : "sorted", c.tune_ms[0], c.tune_ms[1], c.tune_ms[2],
+                     c.tune_ms[3]);
             s += buf;
         }
         s += "]}";

@@ -157,6 +157,11 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TRY(alloc(&err, 1));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
         CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        if (sizeof(T) == 4 && (lag_try<0>() || lag_try<1>() || lag_try<2>())) {
+            CONAN_TRY(alloc(&lacc, mf.cells));
+            CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st));
+            dep_variant = DEP_LAG;
+        }
         CONAN_TRY(fft.create(mf, sizeof(T) == 8, batch));
         CONAN_TRY(alloc((char **)&work, fft.work_bytes));
         CONAN_TRY(fft.bind(work, st));
@@ -185,7 +190,87 @@ template <typename T, int R> struct PM : PMBase {
     dim3 grid_p() const { return dim3((unsigned)((np + 255) / 256)); }
 
     // --- deposit ---------------------------------------------------------
-    int dep_variant = 0;  // tile shape and block size (DepTile<R, V>), chosen by the autotuner
+    // 0 .. DEP_VARIANTS-1: sorted deposit with tile shape DepTile<R, V>;
+    // DEP_LAG: Lagrangian-window deposit (FP32). Chosen by the autotuner.
+    static constexpr int DEP_LAG = DEP_VARIANTS;
+    int dep_variant = 0;
+
+    // Lagrangian deposit: accumulator mesh, lattice-tile variant and window.
+    unsigned long long *lacc = nullptr;
+    int lag_v = -1;  // LagTile<R, V> variant that fits this mesh, -1: none
+    LagWin lwin{};
+    size_t lag_smem = 0;
+
+    bool lag_on() const { return sizeof(T) == 4 && dep_variant == DEP_LAG && lag_v >= 0 && lacc; }
+
+    template <int V> bool lag_try() {
+        typedef LagTile<R, V> L;
+        const int n = mm.n;
+        if (n < L::LX || (R >= 2 && n < L::LY) || (R == 3 && n < L::LZ)) return false;
+        LagWin w{};
+        w.w[0] = L::LX * prm.f + L::M;
+        w.w[1] = R >= 2 ? L::LY * prm.f + L::M : 1;
+        w.w[2] = R == 3 ? L::LZ * prm.f + L::M : 1;
+        w.cells = (w.w[0] * w.w[1] * w.w[2] + 3) & ~3;
+        size_t sh = (size_t)w.cells * 2 * sizeof(uint32_t);
+        if (sh > 112 * 1024) return false;
+        if constexpr (sizeof(T) == 4) {  // set once here, outside any stream capture
+            auto kern = k_deposit_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+        }
+        lwin = w;
+        lag_smem = sh;
+        lag_v = V;
+        return true;
+    }
+
+    template <int V> int launch_lag() {
+        if constexpr (sizeof(T) == 4) {
+            typedef LagTile<R, V> L;
+            size_t tiles = (size_t)(mm.n / L::LX) * (R >= 2 ? mm.n / L::LY : 1) * (R == 3 ? mm.n / L::LZ : 1) *
+                           (size_t)mm.batch;
+            auto kern = k_deposit_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
+            CONAN_TIMED(prof, "deposit", st, (kern<<<(unsigned)tiles, L::THREADS, lag_smem, st>>>(P, mf, lwin, lacc)));
+            return CONAN_OK;
+        } else {
+            return set_error(CONAN_ERR_UNSUPPORTED, "the Lagrangian deposit is FP32 only");
+        }
+    }
+
+    int deposit_lag() {
+        if (lag_v == 0) CONAN_TRY(launch_lag<0>());
+        else if (lag_v == 1) CONAN_TRY(launch_lag<1>());
+        else CONAN_TRY(launch_lag<2>());
+        size_t nt = (mf.cells + 1) / 2;
+        CONAN_TIMED(prof, "deposit_mesh", st,
+                    (k_acc_mesh<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lacc, mesh, mf.cells, mass)));
+        mesh_holds = 1;
+        return CONAN_OK;
+    }
+
+    // CONAN_DEPOSIT_SORTED or CONAN_DEPOSIT_LAGRANGIAN.
+    int set_deposit(int mode) override {
+        if (mode == CONAN_DEPOSIT_SORTED) {
+            dep_variant = 0;
+            return CONAN_OK;
+        }
+        if (mode == CONAN_DEPOSIT_LAGRANGIAN) {
+            if (sizeof(T) != 4 || lag_v < 0 || !lacc)
+                return set_error(CONAN_ERR_UNSUPPORTED,
+                                 "the Lagrangian deposit needs FP32 and a lattice of at least one tile per axis");
+            dep_variant = DEP_LAG;
+            return CONAN_OK;
+        }
+        return set_error(CONAN_ERR_ARG, "unknown deposit mode %d", mode);
+    }
+    int get_deposit(int *mode) override {
+        if (!mode) return set_error(CONAN_ERR_ARG, "null mode");
+        *mode = lag_on() ? CONAN_DEPOSIT_LAGRANGIAN : CONAN_DEPOSIT_SORTED;
+        return CONAN_OK;
+    }
 
     // Tiled deposit with tile variant V; returns 1 when V does not fit the
     // mesh (the caller falls back), CONAN_OK or an error code.
@@ -211,6 +296,7 @@ template <typename T, int R> struct PM : PMBase {
     }
 
     int deposit() {
+        if (lag_on()) return deposit_lag();
         if (!ranks_pending) CONAN_TRY(rank_pass());
         size_t nb = (mf.cells + SCAN_CHUNK - 1) / SCAN_CHUNK;
         CONAN_TIMED(prof, "scan", st,
@@ -238,7 +324,8 @@ template <typename T, int R> struct PM : PMBase {
 
     // --- Poisson: mesh (delta) -> mesh (phi) [and gradient meshes] ------
     int poisson(double a) {
-        double gs = -G / (a * (double)mf.cells) * std::pow(prm.size / (2 * M_PI), 2);
+        // per-member normalisation: 1 / (cells of one box)
+        double gs = -G / (a * (double)((size_t)1 << mf.cshift)) * std::pow(prm.size / (2 * M_PI), 2);
         unsigned gb = (unsigned)((mf.spec + 255) / 256);
         CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
         CONAN_TIMED(prof, "green", st, (k_green<T><<<gb, 256, 0, st>>>(spec, mf, (T)gs)));
@@ -257,8 +344,12 @@ template <typename T, int R> struct PM : PMBase {
     }
 
     int gkd(bool kick, double ck, bool drift, double cd, bool rank_after) {
-        if (rank_after && ranks_pending)
+        rank_after = rank_after && !lag_on();  // the Lagrangian deposit needs no ranks
+        // ranks of positions about to move are stale either way
+        if ((rank_after || drift) && ranks_pending) {
             CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+            ranks_pending = false;
+        }
         GKD c{ck, cd, kick ? 1 : 0, drift ? 1 : 0, rank_after ? 1 : 0, prm.periodic_gather ? 1 : 0};
         const char *name = kick ? (drift ? "gather_kick_drift" : "gather_kick") : "drift";
         if (prm.gradient == CONAN_GRAD_SPECTRAL)
@@ -629,6 +720,14 @@ int conan_pm_kick(conan_pm *h, double a, double da) {
 int conan_pm_set_callback_interval(conan_pm *h, unsigned k) {
     H_GUARD(h);
     return h->impl->set_cb_every(k);
+}
+int conan_pm_set_deposit(conan_pm *h, int mode) {
+    H_GUARD(h);
+    return h->impl->set_deposit(mode);
+}
+int conan_pm_get_deposit(conan_pm *h, int *mode) {
+    H_GUARD(h);
+    return h->impl->get_deposit(mode);
 }
 int conan_pm_run(conan_pm *h, const double *phi, double a0, double da, unsigned n, conan_step_cb cb,
                  void *user) {

@@ -34,6 +34,8 @@ struct PMBase {
     virtual int device_bytes(size_t *b) = 0;
     virtual int sync() = 0;
     virtual int set_cb_every(unsigned k) = 0;
+    virtual int set_deposit(int mode) = 0;
+    virtual int get_deposit(int *mode) = 0;
     virtual int device() const = 0;
     virtual void *stream() const = 0;
 };

@@ -232,6 +232,19 @@ class Gravity:
     def sync(self):
         L.check(L.lib().conan_pm_sync(self._h))
 
+    @property
+    def deposit_mode(self) -> str:
+        """"sorted" (counting sort + tiled reduction) or "lagrangian"
+        (lattice tiles into shared-memory windows, FP32)."""
+        m = C.c_int()
+        L.check(L.lib().conan_pm_get_deposit(self._h, C.byref(m)))
+        return "lagrangian" if m.value == L.DEPOSIT_LAGRANGIAN else "sorted"
+
+    @deposit_mode.setter
+    def deposit_mode(self, mode: str):
+        L.check(L.lib().conan_pm_set_deposit(self._h, {"sorted": L.DEPOSIT_SORTED,
+                                                       "lagrangian": L.DEPOSIT_LAGRANGIAN}[mode]))
+
     def stream_ptr(self) -> int:
         """The handle's cudaStream_t as an integer (torch.cuda.ExternalStream)."""
         s = C.c_void_p()

@@ -145,6 +145,19 @@ typedef int (*conan_step_cb)(conan_pm *h, unsigned step, double a, void *user);
  * CUDA graph with the kick of one step fused to the drift of the next. */
 int conan_pm_set_callback_interval(conan_pm *h, unsigned k);
 
+/* Deposit algorithm of the handle (both give the same density, bit for bit,
+ * in FP32; md_cic, src/run/numeric.hh:106-139, in both cases):
+ * CONAN_DEPOSIT_SORTED      counting sort by cell, tiled integer reduction
+ *                           (FP32 and FP64);
+ * CONAN_DEPOSIT_LAGRANGIAN  lattice tiles summed into shared-memory windows
+ *                           of integer slots, then into an integer mesh
+ *                           (FP32, the FP32 default when the lattice holds
+ *                           one tile per axis; CONAN_ERR_UNSUPPORTED else). */
+#define CONAN_DEPOSIT_SORTED 0
+#define CONAN_DEPOSIT_LAGRANGIAN 1
+int conan_pm_set_deposit(conan_pm *h, int mode);
+int conan_pm_get_deposit(conan_pm *h, int *mode);
+
 /* LeapFrog::run, src/run/leapfrog.hh:33-46: init from phi (if phi is not
  * NULL) at (a0, a0 + da/2), then n x (drift(a, da); kick(a + da/2, da);
  * a += da; cb(i, a)). */

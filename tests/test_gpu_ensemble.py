@@ -46,7 +46,8 @@ def test_graph_run_repeats_and_autotuner_reports(gpu, conan):
     d = e.describe()
     assert len(d["classes"]) == 2
     for c in d["classes"]:
-        assert 0 <= c["deposit_variant"] < 3
+        assert 0 <= c["deposit_variant"] <= 3  # 3: Lagrangian
+        assert c["deposit"] in ("sorted", "lagrangian")
     assert e.total_particles() == 3 * 32 ** 3 + 2 * 16 ** 3
     e.close()
 

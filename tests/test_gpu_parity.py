@@ -81,6 +81,59 @@ def test_deposit_matches_md_cic(gpu, conan, oracle, dim, Nm, f, prec, tol):
     g.close()
 
 
+@pytest.mark.parametrize("dim,Nm,f,amp", [(3, 32, 1, 3.0), (3, 64, 1, 12.0), (3, 16, 2, 3.0), (3, 8, 2, 6.0),
+                                          (2, 64, 1, 20.0), (2, 32, 2, 3.0), (2, 16, 1, 2.0), (1, 1024, 1, 50.0),
+                                          (1, 128, 2, 9.0), (3, 32, 1, 400.0), (2, 64, 1, 5000.0)])
+def test_lagrangian_deposit_equals_sorted_bit_for_bit(gpu, conan, dim, Nm, f, amp):
+    """Both FP32 deposits sum the same integer corner weights, so the
+    densities are identical, also for tiles stretched far beyond their
+    shared-memory window (amp in force cells: particles leave the window,
+    cross the periodic boundary, or land anywhere in the box)."""
+    X, Pm = _particles(dim, Nm, f, 40.0, amp, 7)
+    g = conan.Gravity(dim, Nm, f, 40.0, precision="fp32")
+    assert g.deposit_mode == "lagrangian"
+    g.set_state(X, Pm, 0.1, 0.1)
+    lag = g.density()
+    g.deposit_mode = "sorted"
+    srt = g.density()
+    assert np.array_equal(lag, srt)
+    g.deposit_mode = "lagrangian"
+    assert np.array_equal(lag, g.density())  # the accumulator was cleared
+    g.close()
+
+
+def test_deposit_modes_give_identical_runs(gpu, conan, oracle):
+    dim, mbits, L = 3, 5, 64.0
+    Nm = 1 << mbits
+    noise = oracle.noise_mt19937(11, Nm ** dim)
+    phi = oracle.potential(dim, mbits, L, oracle.grf_scale_free(dim, mbits, L, -2, True, 2.0, 0.83, noise))
+    out = []
+    for mode in ("lagrangian", "sorted"):
+        g = conan.Gravity(dim, Nm, 1, L)
+        g.deposit_mode = mode
+        g.run(phi, 0.05, 0.0475, 8)
+        out.append(g.state())
+        g.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    # switching between steps: the sorted deposit must not reuse stale ranks
+    g = conan.Gravity(dim, Nm, 1, L)
+    conan.LeapFrog(0.05, 0.0475, 4).run(g, phi)
+    g.deposit_mode = "sorted"
+    for i in range(4, 8):
+        a = 0.05 + i * 0.0475
+        g.drift(a, 0.0475)
+        g.kick(a + 0.0475 / 2, 0.0475)
+        g.deposit_mode = "lagrangian" if i % 2 else "sorted"
+    X, P = g.state()
+    assert np.array_equal(X, out[0][0]) and np.array_equal(P, out[0][1])
+    g.close()
+    g = conan.Gravity(dim, Nm, 1, L, precision="fp64")
+    assert g.deposit_mode == "sorted"
+    with pytest.raises(conan.ConanError):
+        g.deposit_mode = "lagrangian"
+    g.close()
+
+
 @pytest.mark.parametrize("dim,Nm,f", [(2, 64, 1), (3, 32, 1), (3, 16, 2), (1, 64, 2)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 3e-4)])
 def test_kick_and_drift_match_reference(gpu, conan, oracle, dim, Nm, f, prec, tol):
