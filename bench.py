@@ -281,6 +281,18 @@ def run_ours(args):
             "unit": "GB/s", "peak_source": hbm_src, "traffic": None,
             "algorithmic_bytes_per_launch": ab, "ms_per_launch": dom_ms}
     roof["frac"] = roof["achieved"] / hbm
+    # the two rows the target names, each with every kernel it needs per step:
+    # deposit = sort + reduce (sorted) or window deposit + accumulator
+    # conversion (Lagrangian); gather = gradient mesh + gather/kick/drift
+    rows = {}
+    for row, ks, ab_row in (("deposit", ("rank", "scan", "scatter", "deposit", "deposit_mesh"), 12 * Np + 4 * Nc),
+                            ("gather", ("fd_grad", "gather_kick_drift", "gather_kick", "drift"), 48 * Np + 4 * Nc)):
+        t = sum(prof[k][1] for k in ks if k in prof) / args.steps
+        if t > 0:
+            rows[row] = {"kernels": [k for k in ks if k in prof], "ms_per_step": t,
+                         "algorithmic_bytes": ab_row, "achieved": ab_row / (t * 1e-3) / 1e9,
+                         "frac": ab_row / (t * 1e-3) / 1e9 / hbm}
+    roof["rows"] = rows
     step_bytes = 60 * Np + 24 * Nc
     kernels = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(
         x[1] for x in prof.values())), 4)} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}

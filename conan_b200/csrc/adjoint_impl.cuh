@@ -361,6 +361,7 @@ template <typename T, int R> struct Diff : DiffBase {
         return CONAN_OK;
     }
     int load_ckpt(unsigned slot) {
+        CONAN_TRY(pm.positions_reset());
         for (int k = 0; k < R; ++k) {
             CONAN_CUDA(cudaMemcpyAsync(pm.P.d[k], ckpt[slot * 2 * R + k], pm.np * sizeof(T), cudaMemcpyDeviceToDevice,
                                        pm.st));
@@ -385,8 +386,7 @@ template <typename T, int R> struct Diff : DiffBase {
         }
         k_zeldovich<T, R><<<gp(), 256, 0, st>>>(pm.P, ict, mm, cdz(), cpz());
         CONAN_LAUNCHED();
-        if (pm.ranks_pending) CONAN_CUDA(cudaMemsetAsync(pm.count, 0, pm.mf.cells * sizeof(uint32_t), st));
-        pm.ranks_pending = false;
+        CONAN_TRY(pm.positions_reset());
         pm.a_pos = prm.a0;
         pm.a_mom = prm.a0 + prm.da / 2;
         return CONAN_OK;

@@ -168,6 +168,7 @@ template <typename T, int R> struct Ens : EnsBase {
     }
     int load_state(Cls &c) {
         auto &pm = c.d->pm;
+        CONAN_TRY(pm.positions_reset());
         for (int k = 0; k < R; ++k) {
             CONAN_CUDA(cudaMemcpyAsync(pm.P.d[k], c.s0[k], pm.np * sizeof(T), cudaMemcpyDeviceToDevice, pm.st));
             CONAN_CUDA(cudaMemcpyAsync(pm.P.p[k], c.s0[R + k], pm.np * sizeof(T), cudaMemcpyDeviceToDevice, pm.st));

@@ -240,11 +240,45 @@ template <typename T, int R> struct PM : PMBase {
         }
     }
 
+    // The fused gather/kick/drift + deposit of variant V (FP32, FD4).
+    template <int V> int launch_gkd_lag(const GKD &c, const char *name) {
+        if constexpr (sizeof(T) == 4) {
+            typedef LagTile<R, V> L;
+            size_t tiles = (size_t)(mm.n / L::LX) * (R >= 2 ? mm.n / L::LY : 1) * (R == 3 ? mm.n / L::LZ : 1) *
+                           (size_t)mm.batch;
+            auto kern = k_gkd_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
+            CONAN_TIMED(prof, name, st,
+                        (kern<<<(unsigned)tiles, L::THREADS, lag_smem, st>>>(P, mf, grad, c, lwin, lacc)));
+            return CONAN_OK;
+        } else {
+            return set_error(CONAN_ERR_UNSUPPORTED, "the Lagrangian deposit is FP32 only");
+        }
+    }
+
+    // lag_ready: the accumulator holds the deposit of the current positions,
+    // made by the fused kernel and not yet turned into the density mesh.
+    bool lag_ready = false;
+    int drop_lag_deposit() {
+        if (lag_ready) CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st));
+        lag_ready = false;
+        return CONAN_OK;
+    }
+
+    // Particle positions were replaced: ranks and a fused deposit are stale.
+    int positions_reset() {
+        if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
+        ranks_pending = false;
+        return drop_lag_deposit();
+    }
+
     int deposit_lag() {
-        if (lag_v == 0) CONAN_TRY(launch_lag<0>());
-        else if (lag_v == 1) CONAN_TRY(launch_lag<1>());
-        else CONAN_TRY(launch_lag<2>());
-        size_t nt = (mf.cells + 1) / 2;
+        if (!lag_ready) {
+            if (lag_v == 0) CONAN_TRY(launch_lag<0>());
+            else if (lag_v == 1) CONAN_TRY(launch_lag<1>());
+            else CONAN_TRY(launch_lag<2>());
+        }
+        lag_ready = false;
+        size_t nt = (mf.cells + 3) / 4;  // four cells per thread
         CONAN_TIMED(prof, "deposit_mesh", st,
                     (k_acc_mesh<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lacc, mesh, mf.cells, mass)));
         mesh_holds = 1;
@@ -253,6 +287,7 @@ template <typename T, int R> struct PM : PMBase {
 
     // CONAN_DEPOSIT_SORTED or CONAN_DEPOSIT_LAGRANGIAN.
     int set_deposit(int mode) override {
+        CONAN_TRY(drop_lag_deposit());  // a pending fused deposit belongs to the old mode
         if (mode == CONAN_DEPOSIT_SORTED) {
             dep_variant = 0;
             return CONAN_OK;
@@ -343,15 +378,28 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
+    // Kick and/or drift of every particle. rank_after: prepare the next
+    // deposit (counting-sort ranks, or with the Lagrangian deposit and a
+    // drift, the deposit itself in the same kernel).
     int gkd(bool kick, double ck, bool drift, double cd, bool rank_after) {
+        const bool fuse = rank_after && drift && lag_on() && prm.gradient == CONAN_GRAD_FD4;
         rank_after = rank_after && !lag_on();  // the Lagrangian deposit needs no ranks
         // ranks of positions about to move are stale either way
         if ((rank_after || drift) && ranks_pending) {
             CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
             ranks_pending = false;
         }
+        if (drift) CONAN_TRY(drop_lag_deposit());
         GKD c{ck, cd, kick ? 1 : 0, drift ? 1 : 0, rank_after ? 1 : 0, prm.periodic_gather ? 1 : 0};
         const char *name = kick ? (drift ? "gather_kick_drift" : "gather_kick") : "drift";
+        if (fuse) {
+            const char *fname = kick ? "gather_kick_drift_deposit" : "drift_deposit";
+            if (lag_v == 0) CONAN_TRY(launch_gkd_lag<0>(c, fname));
+            else if (lag_v == 1) CONAN_TRY(launch_gkd_lag<1>(c, fname));
+            else CONAN_TRY(launch_gkd_lag<2>(c, fname));
+            lag_ready = true;
+            return CONAN_OK;
+        }
         if (prm.gradient == CONAN_GRAD_SPECTRAL)
             CONAN_TIMED(prof, name, st,
                         (k_gkd<T, R, true><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], grad, c,
@@ -380,8 +428,7 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TIMED(prof, "convert", st, (k_convert<double, T><<<gb, 256, 0, st>>>(xfer, mesh, mm.cells, 1.0, 0.0)));
         double cdz = -apos / (res_m * res_f), cpz = -amom / (res_m * res_f);
         CONAN_TIMED(prof, "zeldovich", st, (k_zeldovich<T, R><<<grid_p(), 256, 0, st>>>(P, mesh, mm, cdz, cpz)));
-        if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
-        ranks_pending = false;
+        CONAN_TRY(positions_reset());
         mesh_holds = 0;
         a_pos = apos;
         a_mom = amom;
@@ -502,8 +549,7 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_CUDA(cudaMemcpyAsync(xfer, X, n * sizeof(double), cudaMemcpyHostToDevice, st));
         CONAN_CUDA(cudaMemcpyAsync(xfer + n, Pm, n * sizeof(double), cudaMemcpyHostToDevice, st));
         CONAN_TIMED(prof, "import", st, (k_import<T, R><<<grid_p(), 256, 0, st>>>(P, res_f, xfer, xfer + n)));
-        if (ranks_pending) CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
-        ranks_pending = false;
+        CONAN_TRY(positions_reset());
         a_pos = apos;
         a_mom = amom;
         CONAN_CUDA(cudaStreamSynchronize(st));

@@ -619,183 +619,6 @@ __global__ void k_deposit_pull(const uint32_t *__restrict__ off,
 
 // ------------------------------------------------------------ Poisson --
 
-// ------------------------------------------------ Lagrangian deposit --
-//
-// FP32 deposit without the sort. One CTA takes a tile of the particle
-// lattice (particles are stored in lattice order, so its loads are
-// coalesced), finds the bounding box of the tile's current cells, and sums
-// the quantised corner weights of every particle into a shared-memory window
-// of the force mesh placed over that box (64-bit integer slots). The window is
-// then added into a 64-bit integer accumulator mesh, one add per non-empty
-// cell; a particle whose corners leave the window (a tile stretched wider
-// than the window) adds its corners to the accumulator directly. Every sum is
-// an integer sum, so the density does not depend on the order of the adds
-// and equals the sorted deposit bit for bit (same fractions, same quantised
-// weights, same final scaling). k_acc_mesh turns the accumulator into the
-// density contrast and clears it for the next deposit.
-
-// Window of the Lagrangian deposit: w[k] force cells along axis k (1 beyond
-// R); cells = w0 w1 w2 rounded up to a multiple of 4.
-struct LagWin {
-    int w[3];
-    int cells;
-};
-
-// Lattice tile (LX x LY x LZ particles), threads and window margin M (cells
-// beyond the tile's own f*L cells, split over both sides) of variant V.
-constexpr int LAG_VARIANTS = 3;
-template <int R, int V> struct LagTile;
-template <> struct LagTile<3, 0> { static constexpr int LX = 32, LY = 8, LZ = 8, THREADS = 512, M = 8; };
-template <> struct LagTile<3, 1> { static constexpr int LX = 16, LY = 8, LZ = 8, THREADS = 256, M = 8; };
-template <> struct LagTile<3, 2> { static constexpr int LX = 8, LY = 8, LZ = 8, THREADS = 128, M = 8; };
-template <> struct LagTile<2, 0> { static constexpr int LX = 64, LY = 32, LZ = 1, THREADS = 512, M = 16; };
-template <> struct LagTile<2, 1> { static constexpr int LX = 32, LY = 16, LZ = 1, THREADS = 128, M = 16; };
-template <> struct LagTile<2, 2> { static constexpr int LX = 16, LY = 16, LZ = 1, THREADS = 64, M = 16; };
-template <> struct LagTile<1, 0> { static constexpr int LX = 2048, LY = 1, LZ = 1, THREADS = 512, M = 64; };
-template <> struct LagTile<1, 1> { static constexpr int LX = 512, LY = 1, LZ = 1, THREADS = 128, M = 64; };
-template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1, THREADS = 32, M = 32; };
-
-template <int R, int LX, int LY, int LZ, int THREADS>
-__global__ void __launch_bounds__(THREADS)
-    k_deposit_lag(Parts<float> P, Mesh m, LagWin win, unsigned long long *__restrict__ acc) {
-    constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
-    static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
-    constexpr int NW = THREADS / 32;
-    extern __shared__ __align__(16) uint32_t lag_sh[];
-    __shared__ int wred[6][NW];
-    __shared__ int org[3];
-    const int cells = win.cells;
-
-    const int s = P.mshift;
-    const int ntx = (1 << s) / LX, nty = R >= 2 ? (1 << s) / LY : 1, ntz = R == 3 ? (1 << s) / LZ : 1;
-    const unsigned tiles = (unsigned)(ntx * nty * ntz);
-    const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
-    const int tx0 = (int)(tile % ntx) * LX;
-    const int ty0 = R >= 2 ? (int)((tile / ntx) % nty) * LY : 0;
-    const int tz0 = R == 3 ? (int)(tile / (ntx * nty)) * LZ : 0;
-    const size_t pbase = (size_t)member << P.bshift;
-    const size_t cb = (size_t)member << m.cshift;
-    const int f = P.f;
-
-    // cells (unwrapped) and 21-bit fractions of this thread's particles
-    int u[NPT][3];
-    uint32_t fr[NPT][3];
-    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-#pragma unroll
-    for (int j = 0; j < NPT; ++j) {
-        const int t = (int)threadIdx.x + j * THREADS;
-        const int lx = t % LX, ly = (t / LX) % LY, lz = t / (LX * LY);
-        const int c[3] = {tx0 + lx, ty0 + ly, tz0 + lz};
-        size_t i = pbase + (size_t)c[0];
-        if (R >= 2) i += (size_t)c[1] << s;
-        if (R == 3) i += (size_t)c[2] << (2 * s);
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            long long Q = __float2ll_rn(__ldg(P.d[k] + i) * 2097152.0f);
-            u[j][k] = c[k] * f + (int)(Q >> 21);
-            fr[j][k] = (uint32_t)(Q & 0x1FFFFF);
-            lo[k] = min(lo[k], u[j][k]);
-            hi[k] = max(hi[k], u[j][k]);
-        }
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        int a = __reduce_min_sync(FULL, lo[k]), b = __reduce_max_sync(FULL, hi[k]);
-        if (lane == 0) {
-            wred[k][wid] = a;
-            wred[3 + k][wid] = b;
-        }
-    }
-    uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
-    for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
-    __syncthreads();
-    if (threadIdx.x < R) {
-        const int k = threadIdx.x;
-        int a = INT_MAX, b = INT_MIN;
-        for (int j = 0; j < NW; ++j) {
-            a = min(a, wred[k][j]);
-            b = max(b, wred[3 + k][j]);
-        }
-        const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
-        // the whole box when it fits (slack split evenly), else centred on it
-        org[k] = ext <= W ? a - (W - ext) / 2 : (int)(((long long)a + b + 1) >> 1) - W / 2;
-    }
-    __syncthreads();
-
-    const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
-    const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2];
-    const int mask = m.n - 1;
-#pragma unroll
-    for (int j = 0; j < NPT; ++j) {
-        float f0 = (float)fr[j][0] * 0x1p-21f;
-        float wx[2] = {1.0f - f0, f0}, wy[2] = {1.0f, 1.0f}, wz[2] = {1.0f, 1.0f};
-        if (R >= 2) {
-            float f1 = (float)fr[j][1] * 0x1p-21f;
-            wy[0] = 1.0f - f1;
-            wy[1] = f1;
-        }
-        if (R == 3) {
-            float f2 = (float)fr[j][2] * 0x1p-21f;
-            wz[0] = 1.0f - f2;
-            wz[1] = f2;
-        }
-        const int l0 = u[j][0] - o0, l1 = R >= 2 ? u[j][1] - o1 : 0, l2 = R == 3 ? u[j][2] - o2 : 0;
-        const bool inside = l0 >= 0 && l0 + 1 < W0 && (R < 2 || (l1 >= 0 && l1 + 1 < W1)) &&
-                            (R < 3 || (l2 >= 0 && l2 + 1 < W2));
-        if (inside) {
-            const int base = (l2 * W1 + l1) * W0 + l0;
-#pragma unroll
-            for (int b = 0; b < (1 << R); ++b) {
-                uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                Slot<float>::add(lag_sh, base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v,
-                                 cells);
-            }
-        } else {
-#pragma unroll
-            for (int b = 0; b < (1 << R); ++b) {
-                uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                size_t g = (size_t)((u[j][0] + (b & 1)) & mask);
-                if (R >= 2) g |= (size_t)((u[j][1] + ((b >> 1) & 1)) & mask) << m.shift;
-                if (R == 3) g |= (size_t)((u[j][2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
-                if (v) atomicAdd(acc + cb + g, (unsigned long long)v);
-            }
-        }
-    }
-    __syncthreads();
-
-    const int wcells = W0 * W1 * W2;
-    for (int c = threadIdx.x; c < wcells; c += THREADS) {
-        uint32_t a = lag_sh[c], b = lag_sh[cells + c];
-        if (a | b) {
-            const int l0 = c % W0, r = c / W0;
-            size_t g = (size_t)((o0 + l0) & mask);
-            if (R >= 2) g |= (size_t)((o1 + r % W1) & mask) << m.shift;
-            if (R == 3) g |= (size_t)((o2 + r / W1) & mask) << (2 * m.shift);
-            atomicAdd(acc + cb + g, ((unsigned long long)b << 32) | a);
-        }
-    }
-}
-
-// Density contrast from the integer accumulator (units of 2^-23 particle
-// weights): out = sum 2^-23 mass - 1, as the sorted deposit; the accumulator
-// is cleared for the next deposit.
-template <typename T>
-__global__ void __launch_bounds__(256) k_acc_mesh(unsigned long long *__restrict__ acc, T *__restrict__ out,
-                                                  size_t n, double scale) {
-    size_t i = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 2;
-    if (i + 1 < n) {
-        ulonglong2 a = *reinterpret_cast<ulonglong2 *>(acc + i);
-        *reinterpret_cast<ulonglong2 *>(acc + i) = make_ulonglong2(0ull, 0ull);
-        out[i] = (T)((double)a.x * 0x1p-23 * scale - 1.0);
-        out[i + 1] = (T)((double)a.y * 0x1p-23 * scale - 1.0);
-    } else if (i < n) {
-        unsigned long long a = acc[i];
-        acc[i] = 0ull;
-        out[i] = (T)((double)a * 0x1p-23 * scale - 1.0);
-    }
-}
-
 // Green's function multiply on the half spectrum: spec *= gs / |n|^2 with
 // gs = -G/(a N_c) (L/2pi)^2, DC = 0 (src/run/nbody.hh:105-110 with
 // Fourier::potential, src/base/fourier.hh:102-109).
@@ -1007,6 +830,270 @@ __global__ void __launch_bounds__(256)
         }
     }
     if (c.rank) rank[i] = atomicAdd(count + cell_base(P, m, i) + deposit_cell<T, R>(P, m, i), 1u);
+}
+
+// ------------------------------------------------ Lagrangian deposit --
+//
+// FP32 deposit without the sort. One CTA takes a tile of the particle
+// lattice (particles are stored in lattice order, so its loads are
+// coalesced), finds the bounding box of the tile's current cells, and sums
+// the quantised corner weights of every particle into a shared-memory window
+// of the force mesh placed over that box (64-bit integer slots). The window is
+// then added into a 64-bit integer accumulator mesh, one add per non-empty
+// cell; a particle whose corners leave the window (a tile stretched wider
+// than the window) adds its corners to the accumulator directly. Every sum is
+// an integer sum, so the density does not depend on the order of the adds
+// and equals the sorted deposit bit for bit (same fractions, same quantised
+// weights, same final scaling). k_acc_mesh turns the accumulator into the
+// density contrast and clears it for the next deposit.
+
+// Window of the Lagrangian deposit: w[k] force cells along axis k (1 beyond
+// R); cells = w0 w1 w2 rounded up to a multiple of 4.
+struct LagWin {
+    int w[3];
+    int cells;
+};
+
+// Lattice tile (LX x LY x LZ particles), threads and window margin M (cells
+// beyond the tile's own f*L cells, split over both sides) of variant V.
+constexpr int LAG_VARIANTS = 3;
+template <int R, int V> struct LagTile;
+template <> struct LagTile<3, 0> { static constexpr int LX = 32, LY = 8, LZ = 8, THREADS = 512, M = 8; };
+template <> struct LagTile<3, 1> { static constexpr int LX = 16, LY = 8, LZ = 8, THREADS = 256, M = 8; };
+template <> struct LagTile<3, 2> { static constexpr int LX = 8, LY = 8, LZ = 8, THREADS = 128, M = 8; };
+template <> struct LagTile<2, 0> { static constexpr int LX = 64, LY = 32, LZ = 1, THREADS = 512, M = 16; };
+template <> struct LagTile<2, 1> { static constexpr int LX = 32, LY = 16, LZ = 1, THREADS = 128, M = 16; };
+template <> struct LagTile<2, 2> { static constexpr int LX = 16, LY = 16, LZ = 1, THREADS = 64, M = 16; };
+template <> struct LagTile<1, 0> { static constexpr int LX = 2048, LY = 1, LZ = 1, THREADS = 512, M = 64; };
+template <> struct LagTile<1, 1> { static constexpr int LX = 512, LY = 1, LZ = 1, THREADS = 128, M = 64; };
+template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1, THREADS = 32, M = 32; };
+
+// The body of the Lagrangian deposit for one lattice tile. FUSED: the
+// particles are first advanced as in k_gkd (gather of the packed gradient,
+// kick, drift; positions and momenta written back) and the new positions are
+// deposited, so the deposit costs no second pass over the particles.
+template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED>
+__device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
+                                         unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
+                                         const GKD &gc) {
+    constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
+    static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
+    constexpr int NW = THREADS / 32;
+    extern __shared__ __align__(16) uint32_t lag_sh[];
+    __shared__ int wred[6][NW];
+    __shared__ int org[3];
+    const int cells = win.cells;
+
+    const int s = P.mshift;
+    const int ntx = (1 << s) / LX, nty = R >= 2 ? (1 << s) / LY : 1, ntz = R == 3 ? (1 << s) / LZ : 1;
+    const unsigned tiles = (unsigned)(ntx * nty * ntz);
+    const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
+    const int tx0 = (int)(tile % ntx) * LX;
+    const int ty0 = R >= 2 ? (int)((tile / ntx) % nty) * LY : 0;
+    const int tz0 = R == 3 ? (int)(tile / (ntx * nty)) * LZ : 0;
+    const size_t pbase = (size_t)member << P.bshift;
+    const size_t cb = (size_t)member << m.cshift;
+    const int f = P.f;
+
+    // displacements of this thread's particles (their cells and fractions
+    // are recomputed from these when depositing) and the box of their cells
+    float dd[NPT][3];
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+#pragma unroll
+    for (int j = 0; j < NPT; ++j) {
+        const int t = (int)threadIdx.x + j * THREADS;
+        const int lx = t % LX, ly = (t / LX) % LY, lz = t / (LX * LY);
+        const int c[3] = {tx0 + lx, ty0 + ly, tz0 + lz};
+        size_t i = pbase + (size_t)c[0];
+        if (R >= 2) i += (size_t)c[1] << s;
+        if (R == 3) i += (size_t)c[2] << (2 * s);
+        float d[3];
+        if constexpr (FUSED) {
+            float p[3];
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                d[k] = P.d[k][i];
+                p[k] = P.p[k][i];
+            }
+            if (gc.kick) {
+                float F[3];
+                gather_force<float, R, false>(P, m, i, nullptr, nullptr, G, gc.periodic, d, F);
+                const float ck = (float)gc.ck;
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    p[k] -= F[k] * ck;
+                    P.p[k][i] = p[k];
+                }
+            }
+            const float cd = (float)gc.cd;
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                d[k] += p[k] * cd;
+                P.d[k][i] = d[k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < R; ++k) d[k] = __ldg(P.d[k] + i);
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            dd[j][k] = d[k];
+            const int uk = c[k] * f + (int)(__float2ll_rn(d[k] * 2097152.0f) >> 21);
+            lo[k] = min(lo[k], uk);
+            hi[k] = max(hi[k], uk);
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        int a = __reduce_min_sync(FULL, lo[k]), b = __reduce_max_sync(FULL, hi[k]);
+        if (lane == 0) {
+            wred[k][wid] = a;
+            wred[3 + k][wid] = b;
+        }
+    }
+    uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
+    for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    if (threadIdx.x < R) {
+        const int k = threadIdx.x;
+        int a = INT_MAX, b = INT_MIN;
+        for (int j = 0; j < NW; ++j) {
+            a = min(a, wred[k][j]);
+            b = max(b, wred[3 + k][j]);
+        }
+        const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
+        // the whole box when it fits (slack split evenly), else centred on it
+        org[k] = ext <= W ? a - (W - ext) / 2 : (int)(((long long)a + b + 1) >> 1) - W / 2;
+    }
+    __syncthreads();
+
+    const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
+    const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2];
+    const int mask = m.n - 1;
+#pragma unroll
+    for (int j = 0; j < NPT; ++j) {
+        // cells (unwrapped) and 21-bit fractions of the deposit position
+        int u[3];
+        uint32_t fr[3];
+        {
+            const int t = (int)threadIdx.x + j * THREADS;
+            const int c[3] = {tx0 + t % LX, ty0 + (t / LX) % LY, tz0 + t / (LX * LY)};
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                long long Q = __float2ll_rn(dd[j][k] * 2097152.0f);
+                u[k] = c[k] * f + (int)(Q >> 21);
+                fr[k] = (uint32_t)(Q & 0x1FFFFF);
+            }
+        }
+        float f0 = (float)fr[0] * 0x1p-21f;
+        float wx[2] = {1.0f - f0, f0}, wy[2] = {1.0f, 1.0f}, wz[2] = {1.0f, 1.0f};
+        if (R >= 2) {
+            float f1 = (float)fr[1] * 0x1p-21f;
+            wy[0] = 1.0f - f1;
+            wy[1] = f1;
+        }
+        if (R == 3) {
+            float f2 = (float)fr[2] * 0x1p-21f;
+            wz[0] = 1.0f - f2;
+            wz[1] = f2;
+        }
+        const int l0 = u[0] - o0, l1 = R >= 2 ? u[1] - o1 : 0, l2 = R == 3 ? u[2] - o2 : 0;
+        const bool inside = l0 >= 0 && l0 + 1 < W0 && (R < 2 || (l1 >= 0 && l1 + 1 < W1)) &&
+                            (R < 3 || (l2 >= 0 && l2 + 1 < W2));
+        if (inside) {
+            const int base = (l2 * W1 + l1) * W0 + l0;
+#pragma unroll
+            for (int b = 0; b < (1 << R); ++b) {
+                uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
+                Slot<float>::add(lag_sh, base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v,
+                                 cells);
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < (1 << R); ++b) {
+                uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
+                size_t g = (size_t)((u[0] + (b & 1)) & mask);
+                if (R >= 2) g |= (size_t)((u[1] + ((b >> 1) & 1)) & mask) << m.shift;
+                if (R == 3) g |= (size_t)((u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+                if (v) atomicAdd(acc + cb + g, (unsigned long long)v);
+            }
+        }
+    }
+    __syncthreads();
+
+    // flush: thread t visits cells t, t + THREADS, ...; the window
+    // coordinates advance incrementally (no divisions in the loop)
+    const int wcells = W0 * W1 * W2;
+    int l0 = (int)threadIdx.x % W0, l1 = ((int)threadIdx.x / W0) % W1, l2 = (int)threadIdx.x / (W0 * W1);
+    const int s0 = THREADS % W0, s1 = (THREADS / W0) % W1, s2 = THREADS / (W0 * W1);
+    for (int c = threadIdx.x; c < wcells; c += THREADS) {
+        uint32_t a = lag_sh[c], b = lag_sh[cells + c];
+        if (a | b) {
+            size_t g = (size_t)((o0 + l0) & mask);
+            if (R >= 2) g |= (size_t)((o1 + l1) & mask) << m.shift;
+            if (R == 3) g |= (size_t)((o2 + l2) & mask) << (2 * m.shift);
+            atomicAdd(acc + cb + g, ((unsigned long long)b << 32) | a);
+        }
+        l0 += s0;
+        l1 += s1;
+        l2 += s2;
+        if (l0 >= W0) {
+            l0 -= W0;
+            ++l1;
+        }
+        if (l1 >= W1) {
+            l1 -= W1;
+            ++l2;
+        }
+    }
+}
+
+template <int R, int LX, int LY, int LZ, int THREADS>
+__global__ void __launch_bounds__(THREADS)
+    k_deposit_lag(Parts<float> P, Mesh m, LagWin win, unsigned long long *__restrict__ acc) {
+    lag_tile<R, LX, LY, LZ, THREADS, false>(P, m, win, acc, nullptr, GKD{});
+}
+
+// Gather + kick + drift of k_gkd (FD4 gradient) fused with the Lagrangian
+// deposit of the drifted positions into the accumulator mesh.
+template <int R, int LX, int LY, int LZ, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+    k_gkd_lag(Parts<float> P, Mesh m, const G4<float> *__restrict__ G, GKD gc, LagWin win,
+              unsigned long long *__restrict__ acc) {
+    lag_tile<R, LX, LY, LZ, THREADS, true>(P, m, win, acc, G, gc);
+}
+
+// Density contrast from the integer accumulator (units of 2^-23 particle
+// weights): out = sum 2^-23 mass - 1, as the sorted deposit; the accumulator
+// is cleared for the next deposit.
+template <typename T>
+__global__ void __launch_bounds__(256) k_acc_mesh(unsigned long long *__restrict__ acc, T *__restrict__ out,
+                                                  size_t n, double scale) {
+    const size_t i = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (i + 3 < n) {  // n is a power of two >= 4 except for tiny meshes
+        ulonglong2 a = *reinterpret_cast<const ulonglong2 *>(acc + i);
+        ulonglong2 b = *reinterpret_cast<const ulonglong2 *>(acc + i + 2);
+        *reinterpret_cast<ulonglong2 *>(acc + i) = make_ulonglong2(0ull, 0ull);
+        *reinterpret_cast<ulonglong2 *>(acc + i + 2) = make_ulonglong2(0ull, 0ull);
+        const double k = 0x1p-23 * scale;
+        T v0 = (T)((double)a.x * k - 1.0), v1 = (T)((double)a.y * k - 1.0);
+        T v2 = (T)((double)b.x * k - 1.0), v3 = (T)((double)b.y * k - 1.0);
+        if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4 *>(out + i) = make_float4(v0, v1, v2, v3);
+        } else {
+            out[i] = v0;
+            out[i + 1] = v1;
+            out[i + 2] = v2;
+            out[i + 3] = v3;
+        }
+    } else {
+        for (size_t j = i; j < n; ++j) {
+            unsigned long long a = acc[j];
+            acc[j] = 0ull;
+            out[j] = (T)((double)a * (0x1p-23 * scale) - 1.0);
+        }
+    }
 }
 
 // ------------------------------------------------------------ init/io --
