@@ -216,7 +216,9 @@ template <typename T, int R> struct PM : PMBase {
         if (sh > 112 * 1024) return false;
         if constexpr (sizeof(T) == 4) {  // set once here, outside any stream capture
             auto kern = k_deposit_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess) {
+            auto fused = k_gkd_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess ||
+                cudaFuncSetAttribute(fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess) {
                 cudaGetLastError();
                 return false;
             }
