@@ -94,6 +94,8 @@ SIGNATURES = {
     "conan_ens_last_ms": (C.c_int, [C.c_void_p, _dp, _dp]),
     "conan_ens_total_particles": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "conan_ens_describe": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "conan_deposit_static": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
 }
 
 

@@ -271,6 +271,32 @@ int conan_ens_total_particles(conan_ens *h, size_t *n);
 /* JSON description of the size classes and the autotuner's choices. */
 int conan_ens_describe(conan_ens *h, char *buf, size_t len);
 
+/* ------------------------------------------------- no-allocation deposit -- */
+
+/* No counterpart in the reference (its md_cic, src/run/numeric.hh:106-139,
+ * is the arithmetic, not the interface). The FP32 CIC density contrast of
+ * conan_pm_density, for callers that may not allocate device memory: a
+ * framework that has already reserved the GPU for its own allocator, a
+ * process with a fixed memory budget, a latency-bound loop that must not
+ * wait on cudaMalloc/cudaFree. Allocates nothing: the integer accumulator is
+ * one static device array of CONAN_DEPOSIT_STATIC_MAX_CELLS 64-bit cells
+ * (16 MiB held by every GPU that loads the library), so meshes of at most
+ * that many cells (128^3, 2048^2) are accepted; larger ones return
+ * CONAN_ERR_ARG.
+ *   d0, d1, d2: device arrays of n_mass^dim FP32 displacements in force-mesh
+ *               cells, particle i at lattice point i (axis 0 fastest), as
+ *               conan_pm stores them (d1, d2 unused below dim 2, 3);
+ *   delta_out:  device array of (f n_mass)^dim floats;
+ *   stream:     cudaStream_t of the work (NULL: the default stream).
+ * The first call on a device looks up the array's address and sets kernel
+ * limits for that device (the device must be current); make it before any
+ * stream capture. All calls on a device share the array: calls whose GPU
+ * work overlaps race; order them on one stream. Each call clears the cells
+ * it uses before depositing. Needs n_mass >= 8 (3D), 16 (2D), 128 (1D). */
+#define CONAN_DEPOSIT_STATIC_MAX_CELLS (1u << 21)
+int conan_deposit_static(int dim, int n_mass, int f, const float *d0, const float *d1, const float *d2,
+                         float *delta_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
