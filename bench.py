@@ -211,8 +211,12 @@ def run_reference_arm(args):
 def algorithmic_bytes(kernel, Np, Nc, fp64):
     """Bytes a kernel must move by definition (FP32; x2 for FP64):
     deposit 12 Np + 4 Nc (positions in, density out); gather+kick+drift
-    48 Np + 4 Nc (positions and momenta in and out, potential in)."""
+    48 Np + 4 Nc (positions and momenta in and out, potential in); the fused
+    gather+kick+drift+deposit kernel does the work of both except writing the
+    density, which its accumulator conversion does: 60 Np + 4 Nc."""
     s = 2 if fp64 else 1
+    if kernel.endswith("_deposit"):
+        return s * (60 * Np + 4 * Nc)
     if kernel.startswith("gather_kick"):
         return s * (48 * Np + 4 * Nc)
     if kernel == "deposit":
@@ -272,7 +276,8 @@ def run_ours(args):
     g32.close()
     # per-kernel profile of the same K steps (CUDA events around every launch)
     gp, msp, _, prof = timed_run("fp32", profile=True)
-    launches = sum(v[0] for k, v in prof.items())
+    # kernels only: cuFFT launches count as library work, the accumulator clear is a memset
+    launches = sum(v[0] for k, v in prof.items() if not k.startswith("fft") and k != "deposit_clear")
     gp.close()
     dom = max((k for k in prof if algorithmic_bytes(k, Np, Nc, False)), key=lambda k: prof[k][1])
     dom_ms = prof[dom][1] / prof[dom][0]
@@ -285,8 +290,13 @@ def run_ours(args):
     # deposit = sort + reduce (sorted) or window deposit + accumulator
     # conversion (Lagrangian); gather = gradient mesh + gather/kick/drift
     rows = {}
-    for row, ks, ab_row in (("deposit", ("rank", "scan", "scatter", "deposit", "deposit_mesh"), 12 * Np + 4 * Nc),
-                            ("gather", ("fd_grad", "gather_kick_drift", "gather_kick", "drift"), 48 * Np + 4 * Nc)):
+    dep_b, gat_b = 12 * Np + 4 * Nc, 48 * Np + 4 * Nc
+    fused = any(k.endswith("_deposit") for k in prof)
+    table = ((("gather+deposit", ("fd_grad", "gather_kick_drift_deposit", "drift_deposit", "gather_kick",
+                                  "deposit_mesh", "deposit_clear"), dep_b + gat_b),) if fused else
+             (("deposit", ("rank", "scan", "scatter", "deposit", "deposit_mesh", "deposit_clear"), dep_b),
+              ("gather", ("fd_grad", "gather_kick_drift", "gather_kick", "drift"), gat_b)))
+    for row, ks, ab_row in table:
         t = sum(prof[k][1] for k in ks if k in prof) / args.steps
         if t > 0:
             rows[row] = {"kernels": [k for k in ks if k in prof], "ms_per_step": t,

@@ -283,6 +283,8 @@ template <typename T, int R> struct PM : PMBase {
         size_t nt = (mf.cells + 3) / 4;  // four cells per thread
         CONAN_TIMED(prof, "deposit_mesh", st,
                     (k_acc_mesh<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lacc, mesh, mf.cells, mass)));
+        CONAN_TIMED(prof, "deposit_clear", st,
+                    CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st)));
         mesh_holds = 1;
         return CONAN_OK;
     }

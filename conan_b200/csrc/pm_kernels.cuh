@@ -845,7 +845,7 @@ __global__ void __launch_bounds__(256)
 // an integer sum, so the density does not depend on the order of the adds
 // and equals the sorted deposit bit for bit (same fractions, same quantised
 // weights, same final scaling). k_acc_mesh turns the accumulator into the
-// density contrast and clears it for the next deposit.
+// density contrast; a memset clears it for the next deposit.
 
 // Window of the Lagrangian deposit: w[k] force cells along axis k (1 beyond
 // R); cells = w0 w1 w2 rounded up to a multiple of 4.
@@ -881,7 +881,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(16) uint32_t lag_sh[];
     __shared__ int wred[6][NW];
-    __shared__ int org[3];
+    __shared__ int org[6];  // window origin per axis, then the extent of the box to flush
     const int cells = win.cells;
 
     const int s = P.mshift;
@@ -963,9 +963,12 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             b = max(b, wred[3 + k][j]);
         }
         const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
-        // the whole box when it fits (slack split evenly), else centred on it
-        org[k] = ext <= W ? a - (W - ext) / 2 : (int)(((long long)a + b + 1) >> 1) - W / 2;
+        // the window starts at the box when the box fits (only the box is
+        // flushed), else it is centred on the box (all of it is flushed)
+        org[k] = ext <= W ? a : (int)(((long long)a + b + 1) >> 1) - W / 2;
+        org[3 + k] = ext <= W ? ext : W;
     }
+    if (threadIdx.x >= R && threadIdx.x < 3) org[3 + threadIdx.x] = 1;
     __syncthreads();
 
     const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
@@ -1022,13 +1025,16 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     }
     __syncthreads();
 
-    // flush: thread t visits cells t, t + THREADS, ...; the window
-    // coordinates advance incrementally (no divisions in the loop)
-    const int wcells = W0 * W1 * W2;
-    int l0 = (int)threadIdx.x % W0, l1 = ((int)threadIdx.x / W0) % W1, l2 = (int)threadIdx.x / (W0 * W1);
-    const int s0 = THREADS % W0, s1 = (THREADS / W0) % W1, s2 = THREADS / (W0 * W1);
-    for (int c = threadIdx.x; c < wcells; c += THREADS) {
-        uint32_t a = lag_sh[c], b = lag_sh[cells + c];
+    // flush the box E0 x E1 x E2 at the window's origin: thread t visits box
+    // cells t, t + THREADS, ...; the coordinates advance incrementally (no
+    // divisions in the loop)
+    const int E0 = org[3], E1 = org[4], E2 = org[5];
+    const int ecells = E0 * E1 * E2;
+    int l0 = (int)threadIdx.x % E0, l1 = ((int)threadIdx.x / E0) % E1, l2 = (int)threadIdx.x / (E0 * E1);
+    const int s0 = THREADS % E0, s1 = (THREADS / E0) % E1, s2 = THREADS / (E0 * E1);
+    for (int c = threadIdx.x; c < ecells; c += THREADS) {
+        const int wc = (l2 * W1 + l1) * W0 + l0;
+        uint32_t a = lag_sh[wc], b = lag_sh[cells + wc];
         if (a | b) {
             size_t g = (size_t)((o0 + l0) & mask);
             if (R >= 2) g |= (size_t)((o1 + l1) & mask) << m.shift;
@@ -1038,12 +1044,12 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
         l0 += s0;
         l1 += s1;
         l2 += s2;
-        if (l0 >= W0) {
-            l0 -= W0;
+        if (l0 >= E0) {
+            l0 -= E0;
             ++l1;
         }
-        if (l1 >= W1) {
-            l1 -= W1;
+        if (l1 >= E1) {
+            l1 -= E1;
             ++l2;
         }
     }
@@ -1065,8 +1071,9 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 }
 
 // Density contrast from the integer accumulator (units of 2^-23 particle
-// weights): out = sum 2^-23 mass - 1, as the sorted deposit; the accumulator
-// is cleared for the next deposit.
+// weights): out = sum 2^-23 mass - 1, as the sorted deposit. The caller
+// clears the accumulator afterwards (a plain memset streams faster than
+// zero stores mixed into this read stream).
 template <typename T>
 __global__ void __launch_bounds__(256) k_acc_mesh(unsigned long long *__restrict__ acc, T *__restrict__ out,
                                                   size_t n, double scale) {
@@ -1074,8 +1081,6 @@ __global__ void __launch_bounds__(256) k_acc_mesh(unsigned long long *__restrict
     if (i + 3 < n) {  // n is a power of two >= 4 except for tiny meshes
         ulonglong2 a = *reinterpret_cast<const ulonglong2 *>(acc + i);
         ulonglong2 b = *reinterpret_cast<const ulonglong2 *>(acc + i + 2);
-        *reinterpret_cast<ulonglong2 *>(acc + i) = make_ulonglong2(0ull, 0ull);
-        *reinterpret_cast<ulonglong2 *>(acc + i + 2) = make_ulonglong2(0ull, 0ull);
         const double k = 0x1p-23 * scale;
         T v0 = (T)((double)a.x * k - 1.0), v1 = (T)((double)a.y * k - 1.0);
         T v2 = (T)((double)b.x * k - 1.0), v3 = (T)((double)b.y * k - 1.0);
@@ -1088,11 +1093,7 @@ __global__ void __launch_bounds__(256) k_acc_mesh(unsigned long long *__restrict
             out[i + 3] = v3;
         }
     } else {
-        for (size_t j = i; j < n; ++j) {
-            unsigned long long a = acc[j];
-            acc[j] = 0ull;
-            out[j] = (T)((double)a * (0x1p-23 * scale) - 1.0);
-        }
+        for (size_t j = i; j < n; ++j) out[j] = (T)((double)acc[j] * (0x1p-23 * scale) - 1.0);
     }
 }
 
