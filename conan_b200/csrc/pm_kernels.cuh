@@ -719,6 +719,24 @@ __global__ void __launch_bounds__(256) k_fd_grad(const T *__restrict__ phi, G4<T
     G[c] = G4<T>{g[0], g[1], g[2], T(0)};
 }
 
+// CIC interpolation of the packed node gradients: F = sum over the 2^R
+// corners b of prod_k (a1 or a0) times the gradient of corner b, which
+// load(b) returns. One arithmetic for every source of the gradients, so the
+// global-memory and shared-memory gathers agree bit for bit.
+template <typename T, int R, typename LOAD>
+__device__ __forceinline__ void fd4_interp(const T *a1, const T *a0, T *F, LOAD load) {
+#pragma unroll
+    for (int b = 0; b < (1 << R); ++b) {
+        T z = 1;
+#pragma unroll
+        for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
+        G4<T> gv = load(b);
+        F[0] += gv.x * z;
+        if (R > 1) F[1] += gv.y * z;
+        if (R > 2) F[2] += gv.z * z;
+    }
+}
+
 // CIC-interpolated force of particle i: sum over corners of weight times
 // the node gradient (packed FD4 mesh G, or the spectral gradient meshes g[k]).
 template <typename T, int R, bool SPECTRAL>
@@ -752,19 +770,12 @@ __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, 
         // FD4 gradient of the corner nodes from the packed gradient mesh
         // (one 16-byte load per corner for FP32).
         (void)phi;
-#pragma unroll
-        for (int b = 0; b < (1 << R); ++b) {
+        fd4_interp<T, R>(a1, a0, F, [&](int b) {
             uint32_t ci = 0;
 #pragma unroll
             for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
-            T z = 1;
-#pragma unroll
-            for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
-            G4<T> gv = load_g4(G + cb + ci);
-            F[0] += gv.x * z;
-            if (R > 1) F[1] += gv.y * z;
-            if (R > 2) F[2] += gv.z * z;
-        }
+            return load_g4(G + cb + ci);
+        });
     }
 }
 
@@ -895,55 +906,179 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     const size_t cb = (size_t)member << m.cshift;
     const int f = P.f;
 
-    // displacements of this thread's particles (their cells and fractions
-    // are recomputed from these when depositing) and the box of their cells
-    float dd[NPT][3];
-    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-#pragma unroll
-    for (int j = 0; j < NPT; ++j) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    auto pidx = [&](int j, int *c) {  // lattice point and index of the thread's particle j
         const int t = (int)threadIdx.x + j * THREADS;
-        const int lx = t % LX, ly = (t / LX) % LY, lz = t / (LX * LY);
-        const int c[3] = {tx0 + lx, ty0 + ly, tz0 + lz};
+        c[0] = tx0 + t % LX;
+        c[1] = ty0 + (t / LX) % LY;
+        c[2] = tz0 + t / (LX * LY);
         size_t i = pbase + (size_t)c[0];
         if (R >= 2) i += (size_t)c[1] << s;
         if (R == 3) i += (size_t)c[2] << (2 * s);
-        float d[3];
-        if constexpr (FUSED) {
-            float p[3];
+        return i;
+    };
+
+    // displacements of this thread's particles (their cells and fractions
+    // are recomputed from these when depositing)
+    float dd[NPT][3];
+    if constexpr (FUSED) {
+#pragma unroll
+        for (int j = 0; j < NPT; ++j) {
+            int c[3];
+            const size_t i = pidx(j, c);
+#pragma unroll
+            for (int k = 0; k < R; ++k) dd[j][k] = P.d[k][i];
+        }
+        const float ck = (float)gc.ck, cd = (float)gc.cd;
+        bool staged = false;
+        int g0 = 0, g1 = 0, g2 = 0, E0 = 1, E1 = 1;
+        float4 *sg = reinterpret_cast<float4 *>(lag_sh);
+        const int mask = m.n - 1;
+        if (gc.kick) {
+            // Corner origins of the gather (the reference's truncating
+            // origin unless periodic) and the box they span. When the box
+            // of corners fits in shared memory, the tile's packed gradients
+            // are staged there with coalesced loads and every particle
+            // gathers from shared memory; otherwise from global memory.
+            __shared__ int gw[6];
+            int glo[3] = {INT_MAX, INT_MAX, INT_MAX}, ghi[3] = {INT_MIN, INT_MIN, INT_MIN};
+#pragma unroll
+            for (int j = 0; j < NPT; ++j) {
+                int c[3];
+                (void)pidx(j, c);
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    int o;
+                    float a;
+                    gather_axis<float>(dd[j][k], c[k] * f, gc.periodic, &o, &a);
+                    glo[k] = min(glo[k], o);
+                    ghi[k] = max(ghi[k], o);
+                }
+            }
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                d[k] = P.d[k][i];
-                p[k] = P.p[k][i];
+                int a = __reduce_min_sync(FULL, glo[k]), b = __reduce_max_sync(FULL, ghi[k]);
+                if (lane == 0) {
+                    wred[k][wid] = a;
+                    wred[3 + k][wid] = b;
+                }
             }
+            __syncthreads();
+            if (threadIdx.x < 3) {
+                const int k = threadIdx.x;
+                int a = 0, b = 0;
+                if (k < R) {
+                    a = INT_MAX;
+                    b = INT_MIN;
+                    for (int j = 0; j < NW; ++j) {
+                        a = min(a, wred[k][j]);
+                        b = max(b, wred[3 + k][j]);
+                    }
+                }
+                gw[k] = a;
+                gw[3 + k] = b - a + 2;  // corners o .. o + 1
+            }
+            __syncthreads();
+            g0 = gw[0];
+            g1 = gw[1];
+            g2 = gw[2];
+            E0 = gw[3];
+            E1 = R >= 2 ? gw[4] : 1;
+            const int E2 = R == 3 ? gw[5] : 1;
+            const long long gcells = (long long)E0 * E1 * E2;
+            staged = gcells <= (long long)(cells / 2);  // float4 per cell in the window buffer
+            if (staged) {
+                const int ec = (int)gcells;
+                int l0 = (int)threadIdx.x % E0, l1 = ((int)threadIdx.x / E0) % E1, l2 = (int)threadIdx.x / (E0 * E1);
+                const int s0 = THREADS % E0, s1 = (THREADS / E0) % E1, s2 = THREADS / (E0 * E1);
+#pragma unroll 4
+                for (int c = threadIdx.x; c < ec; c += THREADS) {
+                    size_t g = (size_t)((g0 + l0) & mask);
+                    if (R >= 2) g |= (size_t)((g1 + l1) & mask) << m.shift;
+                    if (R == 3) g |= (size_t)((g2 + l2) & mask) << (2 * m.shift);
+                    sg[c] = __ldg(reinterpret_cast<const float4 *>(G + cb + g));
+                    l0 += s0;
+                    l1 += s1;
+                    l2 += s2;
+                    if (l0 >= E0) {
+                        l0 -= E0;
+                        ++l1;
+                    }
+                    if (l1 >= E1) {
+                        l1 -= E1;
+                        ++l2;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // kick (from the staged or the global gradients) and drift
+#pragma unroll
+        for (int j = 0; j < NPT; ++j) {
+            int c[3];
+            const size_t i = pidx(j, c);
+            float p[3];
+#pragma unroll
+            for (int k = 0; k < R; ++k) p[k] = P.p[k][i];
             if (gc.kick) {
-                float F[3];
-                gather_force<float, R, false>(P, m, i, nullptr, nullptr, G, gc.periodic, d, F);
-                const float ck = (float)gc.ck;
+                int o[3];
+                float a1[3], a0[3], F[3];
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    gather_axis<float>(dd[j][k], c[k] * f, gc.periodic, &o[k], &a1[k]);
+                    a0[k] = 1.0f - a1[k];
+                    F[k] = 0.0f;
+                }
+                if (staged) {
+                    const int b0 = ((R == 3 ? o[2] - g2 : 0) * E1 + (R >= 2 ? o[1] - g1 : 0)) * E0 + (o[0] - g0);
+                    fd4_interp<float, R>(a1, a0, F, [&](int b) {
+                        float4 v = sg[b0 + (b & 1) + ((b >> 1) & 1) * E0 + ((b >> 2) & 1) * E0 * E1];
+                        return G4<float>{v.x, v.y, v.z, v.w};
+                    });
+                } else {
+                    fd4_interp<float, R>(a1, a0, F, [&](int b) {
+                        uint32_t ci = 0;
+#pragma unroll
+                        for (int k = R - 1; k >= 0; --k)
+                            ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
+                        return load_g4(G + cb + ci);
+                    });
+                }
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
                     p[k] -= F[k] * ck;
                     P.p[k][i] = p[k];
                 }
             }
-            const float cd = (float)gc.cd;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                d[k] += p[k] * cd;
-                P.d[k][i] = d[k];
+                dd[j][k] += p[k] * cd;
+                P.d[k][i] = dd[j][k];
             }
-        } else {
-#pragma unroll
-            for (int k = 0; k < R; ++k) d[k] = __ldg(P.d[k] + i);
         }
+        if (gc.kick) __syncthreads();  // the buffer becomes the deposit window below
+    } else {
+#pragma unroll
+        for (int j = 0; j < NPT; ++j) {
+            int c[3];
+            const size_t i = pidx(j, c);
+#pragma unroll
+            for (int k = 0; k < R; ++k) dd[j][k] = __ldg(P.d[k] + i);
+        }
+    }
+    // the box of the deposit cells
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+#pragma unroll
+    for (int j = 0; j < NPT; ++j) {
+        int c[3];
+        (void)pidx(j, c);
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            dd[j][k] = d[k];
-            const int uk = c[k] * f + (int)(__float2ll_rn(d[k] * 2097152.0f) >> 21);
+            const int uk = c[k] * f + (int)(__float2ll_rn(dd[j][k] * 2097152.0f) >> 21);
             lo[k] = min(lo[k], uk);
             hi[k] = max(hi[k], uk);
         }
     }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         int a = __reduce_min_sync(FULL, lo[k]), b = __reduce_max_sync(FULL, hi[k]);
