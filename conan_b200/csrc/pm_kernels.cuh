@@ -883,202 +883,121 @@ template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1
 // particles are first advanced as in k_gkd (gather of the packed gradient,
 // kick, drift; positions and momenta written back) and the new positions are
 // deposited, so the deposit costs no second pass over the particles.
+//
+// Thread t handles particles t, t + THREADS, ... of the tile (lattice order,
+// x fastest): every load and store of the particle arrays is coalesced, and
+// the lattice point of each particle follows from t by constant strides. The
+// cell (relative to the tile) and the 21-bit fractions of each deposit
+// position are computed once and kept in registers (fractions packed in two).
 template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED>
 __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
                                          unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
                                          const GKD &gc) {
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
+    static_assert(R != 3 || THREADS % (LX * LY) == 0, "3D blocks cover whole lattice planes");
+    static_assert(R != 2 || THREADS % LX == 0, "2D blocks cover whole lattice rows");
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(16) uint32_t lag_sh[];
     __shared__ int wred[6][NW];
     __shared__ int org[6];  // window origin per axis, then the extent of the box to flush
     const int cells = win.cells;
 
+    // clear the window first: the stores overlap the particle loads below
+    {
+        uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
+        for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    }
+
     const int s = P.mshift;
     const int ntx = (1 << s) / LX, nty = R >= 2 ? (1 << s) / LY : 1, ntz = R == 3 ? (1 << s) / LZ : 1;
     const unsigned tiles = (unsigned)(ntx * nty * ntz);
     const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
-    const int tx0 = (int)(tile % ntx) * LX;
-    const int ty0 = R >= 2 ? (int)((tile / ntx) % nty) * LY : 0;
-    const int tz0 = R == 3 ? (int)(tile / (ntx * nty)) * LZ : 0;
-    const size_t pbase = (size_t)member << P.bshift;
-    const size_t cb = (size_t)member << m.cshift;
     const int f = P.f;
+    // lattice point of the thread's first particle; particle j adds DJ to the
+    // slowest axis of the tile (z in 3D, y in 2D, x in 1D)
+    const int tid = (int)threadIdx.x;
+    int c0[3];
+    c0[0] = (int)(tile % ntx) * LX + (R == 1 ? tid : tid % LX);
+    c0[1] = R >= 2 ? (int)((tile / ntx) % nty) * LY + (R == 2 ? tid / LX : (tid / LX) % LY) : 0;
+    c0[2] = R == 3 ? (int)(tile / (ntx * nty)) * LZ + tid / (LX * LY) : 0;
+    constexpr int DJ = R == 3 ? THREADS / (LX * LY) : R == 2 ? THREADS / LX : THREADS;
+    const int sj = (R - 1) * s;  // shift of the slowest axis in the particle index
+    const size_t i0 = ((size_t)member << P.bshift) + (size_t)c0[0] + (R >= 2 ? (size_t)c0[1] << s : 0) +
+                      (R == 3 ? (size_t)c0[2] << (2 * s) : 0);
+    const size_t cb = (size_t)member << m.cshift;
+    // tile origin in force cells: deposit cells are kept relative to it
+    const int b0 = (c0[0] - (R == 1 ? tid : tid % LX)) * f;
+    const int b1 = R >= 2 ? (c0[1] - (R == 2 ? tid / LX : (tid / LX) % LY)) * f : 0;
+    const int b2 = R == 3 ? (c0[2] - tid / (LX * LY)) * f : 0;
+    const int base[3] = {b0, b1, b2};
 
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    auto pidx = [&](int j, int *c) {  // lattice point and index of the thread's particle j
-        const int t = (int)threadIdx.x + j * THREADS;
-        c[0] = tx0 + t % LX;
-        c[1] = ty0 + (t / LX) % LY;
-        c[2] = tz0 + t / (LX * LY);
-        size_t i = pbase + (size_t)c[0];
-        if (R >= 2) i += (size_t)c[1] << s;
-        if (R == 3) i += (size_t)c[2] << (2 * s);
-        return i;
-    };
-
-    // displacements of this thread's particles (their cells and fractions
-    // are recomputed from these when depositing)
-    float dd[NPT][3];
-    if constexpr (FUSED) {
+    uint32_t pk[NPT][2];  // fractions: fr0 | fr1 << 21, fr1 >> 11 | fr2 << 10
+    int uu[NPT][3];       // deposit cells relative to the tile origin
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    const int mask = m.n - 1;
 #pragma unroll
-        for (int j = 0; j < NPT; ++j) {
-            int c[3];
-            const size_t i = pidx(j, c);
-#pragma unroll
-            for (int k = 0; k < R; ++k) dd[j][k] = P.d[k][i];
-        }
-        const float ck = (float)gc.ck, cd = (float)gc.cd;
-        bool staged = false;
-        int g0 = 0, g1 = 0, g2 = 0, E0 = 1, E1 = 1;
-        float4 *sg = reinterpret_cast<float4 *>(lag_sh);
-        const int mask = m.n - 1;
-        if (gc.kick) {
-            // Corner origins of the gather (the reference's truncating
-            // origin unless periodic) and the box they span. When the box
-            // of corners fits in shared memory, the tile's packed gradients
-            // are staged there with coalesced loads and every particle
-            // gathers from shared memory; otherwise from global memory.
-            __shared__ int gw[6];
-            int glo[3] = {INT_MAX, INT_MAX, INT_MAX}, ghi[3] = {INT_MIN, INT_MIN, INT_MIN};
-#pragma unroll
-            for (int j = 0; j < NPT; ++j) {
-                int c[3];
-                (void)pidx(j, c);
-#pragma unroll
-                for (int k = 0; k < R; ++k) {
-                    int o;
-                    float a;
-                    gather_axis<float>(dd[j][k], c[k] * f, gc.periodic, &o, &a);
-                    glo[k] = min(glo[k], o);
-                    ghi[k] = max(ghi[k], o);
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                int a = __reduce_min_sync(FULL, glo[k]), b = __reduce_max_sync(FULL, ghi[k]);
-                if (lane == 0) {
-                    wred[k][wid] = a;
-                    wred[3 + k][wid] = b;
-                }
-            }
-            __syncthreads();
-            if (threadIdx.x < 3) {
-                const int k = threadIdx.x;
-                int a = 0, b = 0;
-                if (k < R) {
-                    a = INT_MAX;
-                    b = INT_MIN;
-                    for (int j = 0; j < NW; ++j) {
-                        a = min(a, wred[k][j]);
-                        b = max(b, wred[3 + k][j]);
-                    }
-                }
-                gw[k] = a;
-                gw[3 + k] = b - a + 2;  // corners o .. o + 1
-            }
-            __syncthreads();
-            g0 = gw[0];
-            g1 = gw[1];
-            g2 = gw[2];
-            E0 = gw[3];
-            E1 = R >= 2 ? gw[4] : 1;
-            const int E2 = R == 3 ? gw[5] : 1;
-            const long long gcells = (long long)E0 * E1 * E2;
-            staged = gcells <= (long long)(cells / 2);  // float4 per cell in the window buffer
-            if (staged) {
-                const int ec = (int)gcells;
-                int l0 = (int)threadIdx.x % E0, l1 = ((int)threadIdx.x / E0) % E1, l2 = (int)threadIdx.x / (E0 * E1);
-                const int s0 = THREADS % E0, s1 = (THREADS / E0) % E1, s2 = THREADS / (E0 * E1);
-#pragma unroll 4
-                for (int c = threadIdx.x; c < ec; c += THREADS) {
-                    size_t g = (size_t)((g0 + l0) & mask);
-                    if (R >= 2) g |= (size_t)((g1 + l1) & mask) << m.shift;
-                    if (R == 3) g |= (size_t)((g2 + l2) & mask) << (2 * m.shift);
-                    sg[c] = __ldg(reinterpret_cast<const float4 *>(G + cb + g));
-                    l0 += s0;
-                    l1 += s1;
-                    l2 += s2;
-                    if (l0 >= E0) {
-                        l0 -= E0;
-                        ++l1;
-                    }
-                    if (l1 >= E1) {
-                        l1 -= E1;
-                        ++l2;
-                    }
-                }
-                __syncthreads();
-            }
-        }
-        // kick (from the staged or the global gradients) and drift
-#pragma unroll
-        for (int j = 0; j < NPT; ++j) {
-            int c[3];
-            const size_t i = pidx(j, c);
+    for (int j = 0; j < NPT; ++j) {
+        const size_t i = i0 + ((size_t)(j * DJ) << sj);
+        int c[3] = {c0[0], c0[1], c0[2]};
+        c[R - 1] += j * DJ;
+        float d[3];
+        if constexpr (FUSED) {
             float p[3];
 #pragma unroll
-            for (int k = 0; k < R; ++k) p[k] = P.p[k][i];
+            for (int k = 0; k < R; ++k) {
+                d[k] = P.d[k][i];
+                p[k] = P.p[k][i];
+            }
             if (gc.kick) {
                 int o[3];
                 float a1[3], a0[3], F[3];
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
-                    gather_axis<float>(dd[j][k], c[k] * f, gc.periodic, &o[k], &a1[k]);
+                    gather_axis<float>(d[k], c[k] * f, gc.periodic, &o[k], &a1[k]);
                     a0[k] = 1.0f - a1[k];
                     F[k] = 0.0f;
                 }
-                if (staged) {
-                    const int b0 = ((R == 3 ? o[2] - g2 : 0) * E1 + (R >= 2 ? o[1] - g1 : 0)) * E0 + (o[0] - g0);
-                    fd4_interp<float, R>(a1, a0, F, [&](int b) {
-                        float4 v = sg[b0 + (b & 1) + ((b >> 1) & 1) * E0 + ((b >> 2) & 1) * E0 * E1];
-                        return G4<float>{v.x, v.y, v.z, v.w};
-                    });
-                } else {
-                    fd4_interp<float, R>(a1, a0, F, [&](int b) {
-                        uint32_t ci = 0;
+                fd4_interp<float, R>(a1, a0, F, [&](int b) {
+                    uint32_t ci = 0;
 #pragma unroll
-                        for (int k = R - 1; k >= 0; --k)
-                            ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
-                        return load_g4(G + cb + ci);
-                    });
-                }
+                    for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
+                    return load_g4(G + cb + ci);
+                });
+                const float ck = (float)gc.ck;
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
                     p[k] -= F[k] * ck;
                     P.p[k][i] = p[k];
                 }
             }
+            const float cd = (float)gc.cd;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                dd[j][k] += p[k] * cd;
-                P.d[k][i] = dd[j][k];
+                d[k] += p[k] * cd;
+                P.d[k][i] = d[k];
             }
+        } else {
+#pragma unroll
+            for (int k = 0; k < R; ++k) d[k] = __ldg(P.d[k] + i);
         }
-        if (gc.kick) __syncthreads();  // the buffer becomes the deposit window below
-    } else {
-#pragma unroll
-        for (int j = 0; j < NPT; ++j) {
-            int c[3];
-            const size_t i = pidx(j, c);
-#pragma unroll
-            for (int k = 0; k < R; ++k) dd[j][k] = __ldg(P.d[k] + i);
-        }
-    }
-    // the box of the deposit cells
-    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-#pragma unroll
-    for (int j = 0; j < NPT; ++j) {
-        int c[3];
-        (void)pidx(j, c);
+        // deposit cell (unwrapped, relative to the tile origin) and fractions
+        int u[3] = {0, 0, 0};
+        uint32_t fr[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const int uk = c[k] * f + (int)(__float2ll_rn(dd[j][k] * 2097152.0f) >> 21);
-            lo[k] = min(lo[k], uk);
-            hi[k] = max(hi[k], uk);
+            long long Q = __float2ll_rn(d[k] * 2097152.0f);
+            u[k] = c[k] * f - base[k] + (int)(Q >> 21);
+            fr[k] = (uint32_t)(Q & 0x1FFFFF);
+            lo[k] = min(lo[k], u[k]);
+            hi[k] = max(hi[k], u[k]);
         }
+        pk[j][0] = fr[0] | (fr[1] << 21);
+        pk[j][1] = (fr[1] >> 11) | (fr[2] << 10);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) uu[j][k] = u[k];
     }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         int a = __reduce_min_sync(FULL, lo[k]), b = __reduce_max_sync(FULL, hi[k]);
@@ -1087,73 +1006,63 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             wred[3 + k][wid] = b;
         }
     }
-    uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
-    for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
-    if (threadIdx.x < R) {
+    if (threadIdx.x < 3) {
         const int k = threadIdx.x;
-        int a = INT_MAX, b = INT_MIN;
-        for (int j = 0; j < NW; ++j) {
-            a = min(a, wred[k][j]);
-            b = max(b, wred[3 + k][j]);
+        if (k < R) {
+            int a = INT_MAX, b = INT_MIN;
+            for (int j = 0; j < NW; ++j) {
+                a = min(a, wred[k][j]);
+                b = max(b, wred[3 + k][j]);
+            }
+            const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
+            // the window starts at the box when the box fits (only the box
+            // is flushed), else it is centred on the box (all of it flushed)
+            org[k] = ext <= W ? a : (int)(((long long)a + b + 1) >> 1) - W / 2;
+            org[3 + k] = ext <= W ? ext : W;
+        } else {
+            org[k] = 0;
+            org[3 + k] = 1;
         }
-        const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
-        // the window starts at the box when the box fits (only the box is
-        // flushed), else it is centred on the box (all of it is flushed)
-        org[k] = ext <= W ? a : (int)(((long long)a + b + 1) >> 1) - W / 2;
-        org[3 + k] = ext <= W ? ext : W;
     }
-    if (threadIdx.x >= R && threadIdx.x < 3) org[3 + threadIdx.x] = 1;
     __syncthreads();
 
-    const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
+    const int o0 = org[0], o1 = org[1], o2 = org[2];
     const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2];
-    const int mask = m.n - 1;
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
-        // cells (unwrapped) and 21-bit fractions of the deposit position
-        int u[3];
-        uint32_t fr[3];
-        {
-            const int t = (int)threadIdx.x + j * THREADS;
-            const int c[3] = {tx0 + t % LX, ty0 + (t / LX) % LY, tz0 + t / (LX * LY)};
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                long long Q = __float2ll_rn(dd[j][k] * 2097152.0f);
-                u[k] = c[k] * f + (int)(Q >> 21);
-                fr[k] = (uint32_t)(Q & 0x1FFFFF);
-            }
-        }
-        float f0 = (float)fr[0] * 0x1p-21f;
+        const uint32_t fr0 = pk[j][0] & 0x1FFFFFu, fr1 = (pk[j][0] >> 21) | ((pk[j][1] & 0x3FFu) << 11),
+                       fr2 = pk[j][1] >> 10;
+        const int u0 = uu[j][0], u1 = uu[j][1], u2 = uu[j][2];
+        float f0 = (float)fr0 * 0x1p-21f;
         float wx[2] = {1.0f - f0, f0}, wy[2] = {1.0f, 1.0f}, wz[2] = {1.0f, 1.0f};
         if (R >= 2) {
-            float f1 = (float)fr[1] * 0x1p-21f;
+            float f1 = (float)fr1 * 0x1p-21f;
             wy[0] = 1.0f - f1;
             wy[1] = f1;
         }
         if (R == 3) {
-            float f2 = (float)fr[2] * 0x1p-21f;
+            float f2 = (float)fr2 * 0x1p-21f;
             wz[0] = 1.0f - f2;
             wz[1] = f2;
         }
-        const int l0 = u[0] - o0, l1 = R >= 2 ? u[1] - o1 : 0, l2 = R == 3 ? u[2] - o2 : 0;
+        const int l0 = u0 - o0, l1 = R >= 2 ? u1 - o1 : 0, l2 = R == 3 ? u2 - o2 : 0;
         const bool inside = l0 >= 0 && l0 + 1 < W0 && (R < 2 || (l1 >= 0 && l1 + 1 < W1)) &&
                             (R < 3 || (l2 >= 0 && l2 + 1 < W2));
         if (inside) {
-            const int base = (l2 * W1 + l1) * W0 + l0;
+            const int wb = (l2 * W1 + l1) * W0 + l0;
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                Slot<float>::add(lag_sh, base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v,
-                                 cells);
+                Slot<float>::add(lag_sh, wb + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v, cells);
             }
         } else {
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                size_t g = (size_t)((u[0] + (b & 1)) & mask);
-                if (R >= 2) g |= (size_t)((u[1] + ((b >> 1) & 1)) & mask) << m.shift;
-                if (R == 3) g |= (size_t)((u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+                size_t g = (size_t)((b0 + u0 + (b & 1)) & mask);
+                if (R >= 2) g |= (size_t)((b1 + u1 + ((b >> 1) & 1)) & mask) << m.shift;
+                if (R == 3) g |= (size_t)((b2 + u2 + ((b >> 2) & 1)) & mask) << (2 * m.shift);
                 if (v) atomicAdd(acc + cb + g, (unsigned long long)v);
             }
         }
@@ -1165,15 +1074,15 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     // divisions in the loop)
     const int E0 = org[3], E1 = org[4], E2 = org[5];
     const int ecells = E0 * E1 * E2;
-    int l0 = (int)threadIdx.x % E0, l1 = ((int)threadIdx.x / E0) % E1, l2 = (int)threadIdx.x / (E0 * E1);
+    int l0 = tid % E0, l1 = (tid / E0) % E1, l2 = tid / (E0 * E1);
     const int s0 = THREADS % E0, s1 = (THREADS / E0) % E1, s2 = THREADS / (E0 * E1);
-    for (int c = threadIdx.x; c < ecells; c += THREADS) {
+    for (int c = tid; c < ecells; c += THREADS) {
         const int wc = (l2 * W1 + l1) * W0 + l0;
         uint32_t a = lag_sh[wc], b = lag_sh[cells + wc];
         if (a | b) {
-            size_t g = (size_t)((o0 + l0) & mask);
-            if (R >= 2) g |= (size_t)((o1 + l1) & mask) << m.shift;
-            if (R == 3) g |= (size_t)((o2 + l2) & mask) << (2 * m.shift);
+            size_t g = (size_t)((b0 + o0 + l0) & mask);
+            if (R >= 2) g |= (size_t)((b1 + o1 + l1) & mask) << m.shift;
+            if (R == 3) g |= (size_t)((b2 + o2 + l2) & mask) << (2 * m.shift);
             atomicAdd(acc + cb + g, ((unsigned long long)b << 32) | a);
         }
         l0 += s0;
