@@ -719,24 +719,6 @@ __global__ void __launch_bounds__(256) k_fd_grad(const T *__restrict__ phi, G4<T
     G[c] = G4<T>{g[0], g[1], g[2], T(0)};
 }
 
-// CIC interpolation of the packed node gradients: F = sum over the 2^R
-// corners b of prod_k (a1 or a0) times the gradient of corner b, which
-// load(b) returns. One arithmetic for every source of the gradients, so the
-// global-memory and shared-memory gathers agree bit for bit.
-template <typename T, int R, typename LOAD>
-__device__ __forceinline__ void fd4_interp(const T *a1, const T *a0, T *F, LOAD load) {
-#pragma unroll
-    for (int b = 0; b < (1 << R); ++b) {
-        T z = 1;
-#pragma unroll
-        for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
-        G4<T> gv = load(b);
-        F[0] += gv.x * z;
-        if (R > 1) F[1] += gv.y * z;
-        if (R > 2) F[2] += gv.z * z;
-    }
-}
-
 // CIC-interpolated force of particle i: sum over corners of weight times
 // the node gradient (packed FD4 mesh G, or the spectral gradient meshes g[k]).
 template <typename T, int R, bool SPECTRAL>
@@ -770,12 +752,19 @@ __device__ inline void gather_force(const Parts<T> &P, const Mesh &m, size_t i, 
         // FD4 gradient of the corner nodes from the packed gradient mesh
         // (one 16-byte load per corner for FP32).
         (void)phi;
-        fd4_interp<T, R>(a1, a0, F, [&](int b) {
+#pragma unroll
+        for (int b = 0; b < (1 << R); ++b) {
             uint32_t ci = 0;
 #pragma unroll
             for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
-            return load_g4(G + cb + ci);
-        });
+            T z = 1;
+#pragma unroll
+            for (int k = 0; k < R; ++k) z *= ((b >> k) & 1) ? a1[k] : a0[k];
+            G4<T> gv = load_g4(G + cb + ci);
+            F[0] += gv.x * z;
+            if (R > 1) F[1] += gv.y * z;
+            if (R > 2) F[2] += gv.z * z;
+        }
     }
 }
 
@@ -883,64 +872,41 @@ template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1
 // particles are first advanced as in k_gkd (gather of the packed gradient,
 // kick, drift; positions and momenta written back) and the new positions are
 // deposited, so the deposit costs no second pass over the particles.
-//
-// Thread t handles particles t, t + THREADS, ... of the tile (lattice order,
-// x fastest): every load and store of the particle arrays is coalesced, and
-// the lattice point of each particle follows from t by constant strides. The
-// cell (relative to the tile) and the 21-bit fractions of each deposit
-// position are computed once and kept in registers (fractions packed in two).
 template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED>
 __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
                                          unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
                                          const GKD &gc) {
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
-    static_assert(R != 3 || THREADS % (LX * LY) == 0, "3D blocks cover whole lattice planes");
-    static_assert(R != 2 || THREADS % LX == 0, "2D blocks cover whole lattice rows");
     constexpr int NW = THREADS / 32;
     extern __shared__ __align__(16) uint32_t lag_sh[];
     __shared__ int wred[6][NW];
     __shared__ int org[6];  // window origin per axis, then the extent of the box to flush
     const int cells = win.cells;
 
-    // clear the window first: the stores overlap the particle loads below
-    {
-        uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
-        for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
-    }
-
     const int s = P.mshift;
     const int ntx = (1 << s) / LX, nty = R >= 2 ? (1 << s) / LY : 1, ntz = R == 3 ? (1 << s) / LZ : 1;
     const unsigned tiles = (unsigned)(ntx * nty * ntz);
     const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
-    const int f = P.f;
-    // lattice point of the thread's first particle; particle j adds DJ to the
-    // slowest axis of the tile (z in 3D, y in 2D, x in 1D)
-    const int tid = (int)threadIdx.x;
-    int c0[3];
-    c0[0] = (int)(tile % ntx) * LX + (R == 1 ? tid : tid % LX);
-    c0[1] = R >= 2 ? (int)((tile / ntx) % nty) * LY + (R == 2 ? tid / LX : (tid / LX) % LY) : 0;
-    c0[2] = R == 3 ? (int)(tile / (ntx * nty)) * LZ + tid / (LX * LY) : 0;
-    constexpr int DJ = R == 3 ? THREADS / (LX * LY) : R == 2 ? THREADS / LX : THREADS;
-    const int sj = (R - 1) * s;  // shift of the slowest axis in the particle index
-    const size_t i0 = ((size_t)member << P.bshift) + (size_t)c0[0] + (R >= 2 ? (size_t)c0[1] << s : 0) +
-                      (R == 3 ? (size_t)c0[2] << (2 * s) : 0);
+    const int tx0 = (int)(tile % ntx) * LX;
+    const int ty0 = R >= 2 ? (int)((tile / ntx) % nty) * LY : 0;
+    const int tz0 = R == 3 ? (int)(tile / (ntx * nty)) * LZ : 0;
+    const size_t pbase = (size_t)member << P.bshift;
     const size_t cb = (size_t)member << m.cshift;
-    // tile origin in force cells: deposit cells are kept relative to it
-    const int b0 = (c0[0] - (R == 1 ? tid : tid % LX)) * f;
-    const int b1 = R >= 2 ? (c0[1] - (R == 2 ? tid / LX : (tid / LX) % LY)) * f : 0;
-    const int b2 = R == 3 ? (c0[2] - tid / (LX * LY)) * f : 0;
-    const int base[3] = {b0, b1, b2};
+    const int f = P.f;
 
-    uint32_t pk[NPT][2];  // fractions: fr0 | fr1 << 21, fr1 >> 11 | fr2 << 10
-    int uu[NPT][3];       // deposit cells relative to the tile origin
+    // displacements of this thread's particles (their cells and fractions
+    // are recomputed from these when depositing) and the box of their cells
+    float dd[NPT][3];
     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-    const int mask = m.n - 1;
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
-        const size_t i = i0 + ((size_t)(j * DJ) << sj);
-        int c[3] = {c0[0], c0[1], c0[2]};
-        c[R - 1] += j * DJ;
+        const int t = (int)threadIdx.x + j * THREADS;
+        const int lx = t % LX, ly = (t / LX) % LY, lz = t / (LX * LY);
+        const int c[3] = {tx0 + lx, ty0 + ly, tz0 + lz};
+        size_t i = pbase + (size_t)c[0];
+        if (R >= 2) i += (size_t)c[1] << s;
+        if (R == 3) i += (size_t)c[2] << (2 * s);
         float d[3];
         if constexpr (FUSED) {
             float p[3];
@@ -950,20 +916,8 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
                 p[k] = P.p[k][i];
             }
             if (gc.kick) {
-                int o[3];
-                float a1[3], a0[3], F[3];
-#pragma unroll
-                for (int k = 0; k < R; ++k) {
-                    gather_axis<float>(d[k], c[k] * f, gc.periodic, &o[k], &a1[k]);
-                    a0[k] = 1.0f - a1[k];
-                    F[k] = 0.0f;
-                }
-                fd4_interp<float, R>(a1, a0, F, [&](int b) {
-                    uint32_t ci = 0;
-#pragma unroll
-                    for (int k = R - 1; k >= 0; --k) ci = (ci << m.shift) | (uint32_t)((o[k] + ((b >> k) & 1)) & mask);
-                    return load_g4(G + cb + ci);
-                });
+                float F[3];
+                gather_force<float, R, false>(P, m, i, nullptr, nullptr, G, gc.periodic, d, F);
                 const float ck = (float)gc.ck;
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
@@ -981,21 +935,13 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
 #pragma unroll
             for (int k = 0; k < R; ++k) d[k] = __ldg(P.d[k] + i);
         }
-        // deposit cell (unwrapped, relative to the tile origin) and fractions
-        int u[3] = {0, 0, 0};
-        uint32_t fr[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            long long Q = __float2ll_rn(d[k] * 2097152.0f);
-            u[k] = c[k] * f - base[k] + (int)(Q >> 21);
-            fr[k] = (uint32_t)(Q & 0x1FFFFF);
-            lo[k] = min(lo[k], u[k]);
-            hi[k] = max(hi[k], u[k]);
+            dd[j][k] = d[k];
+            const int uk = c[k] * f + (int)(__float2ll_rn(d[k] * 2097152.0f) >> 21);
+            lo[k] = min(lo[k], uk);
+            hi[k] = max(hi[k], uk);
         }
-        pk[j][0] = fr[0] | (fr[1] << 21);
-        pk[j][1] = (fr[1] >> 11) | (fr[2] << 10);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) uu[j][k] = u[k];
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -1006,63 +952,73 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             wred[3 + k][wid] = b;
         }
     }
+    uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
+    for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
-    if (threadIdx.x < 3) {
+    if (threadIdx.x < R) {
         const int k = threadIdx.x;
-        if (k < R) {
-            int a = INT_MAX, b = INT_MIN;
-            for (int j = 0; j < NW; ++j) {
-                a = min(a, wred[k][j]);
-                b = max(b, wred[3 + k][j]);
-            }
-            const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
-            // the window starts at the box when the box fits (only the box
-            // is flushed), else it is centred on the box (all of it flushed)
-            org[k] = ext <= W ? a : (int)(((long long)a + b + 1) >> 1) - W / 2;
-            org[3 + k] = ext <= W ? ext : W;
-        } else {
-            org[k] = 0;
-            org[3 + k] = 1;
+        int a = INT_MAX, b = INT_MIN;
+        for (int j = 0; j < NW; ++j) {
+            a = min(a, wred[k][j]);
+            b = max(b, wred[3 + k][j]);
         }
+        const int W = win.w[k], ext = b - a + 2;  // corners reach hi + 1
+        // the window starts at the box when the box fits (only the box is
+        // flushed), else it is centred on the box (all of it is flushed)
+        org[k] = ext <= W ? a : (int)(((long long)a + b + 1) >> 1) - W / 2;
+        org[3 + k] = ext <= W ? ext : W;
     }
+    if (threadIdx.x >= R && threadIdx.x < 3) org[3 + threadIdx.x] = 1;
     __syncthreads();
 
-    const int o0 = org[0], o1 = org[1], o2 = org[2];
+    const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
     const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2];
+    const int mask = m.n - 1;
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
-        const uint32_t fr0 = pk[j][0] & 0x1FFFFFu, fr1 = (pk[j][0] >> 21) | ((pk[j][1] & 0x3FFu) << 11),
-                       fr2 = pk[j][1] >> 10;
-        const int u0 = uu[j][0], u1 = uu[j][1], u2 = uu[j][2];
-        float f0 = (float)fr0 * 0x1p-21f;
+        // cells (unwrapped) and 21-bit fractions of the deposit position
+        int u[3];
+        uint32_t fr[3];
+        {
+            const int t = (int)threadIdx.x + j * THREADS;
+            const int c[3] = {tx0 + t % LX, ty0 + (t / LX) % LY, tz0 + t / (LX * LY)};
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                long long Q = __float2ll_rn(dd[j][k] * 2097152.0f);
+                u[k] = c[k] * f + (int)(Q >> 21);
+                fr[k] = (uint32_t)(Q & 0x1FFFFF);
+            }
+        }
+        float f0 = (float)fr[0] * 0x1p-21f;
         float wx[2] = {1.0f - f0, f0}, wy[2] = {1.0f, 1.0f}, wz[2] = {1.0f, 1.0f};
         if (R >= 2) {
-            float f1 = (float)fr1 * 0x1p-21f;
+            float f1 = (float)fr[1] * 0x1p-21f;
             wy[0] = 1.0f - f1;
             wy[1] = f1;
         }
         if (R == 3) {
-            float f2 = (float)fr2 * 0x1p-21f;
+            float f2 = (float)fr[2] * 0x1p-21f;
             wz[0] = 1.0f - f2;
             wz[1] = f2;
         }
-        const int l0 = u0 - o0, l1 = R >= 2 ? u1 - o1 : 0, l2 = R == 3 ? u2 - o2 : 0;
+        const int l0 = u[0] - o0, l1 = R >= 2 ? u[1] - o1 : 0, l2 = R == 3 ? u[2] - o2 : 0;
         const bool inside = l0 >= 0 && l0 + 1 < W0 && (R < 2 || (l1 >= 0 && l1 + 1 < W1)) &&
                             (R < 3 || (l2 >= 0 && l2 + 1 < W2));
         if (inside) {
-            const int wb = (l2 * W1 + l1) * W0 + l0;
+            const int base = (l2 * W1 + l1) * W0 + l0;
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                Slot<float>::add(lag_sh, wb + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v, cells);
+                Slot<float>::add(lag_sh, base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v,
+                                 cells);
             }
         } else {
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                size_t g = (size_t)((b0 + u0 + (b & 1)) & mask);
-                if (R >= 2) g |= (size_t)((b1 + u1 + ((b >> 1) & 1)) & mask) << m.shift;
-                if (R == 3) g |= (size_t)((b2 + u2 + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+                size_t g = (size_t)((u[0] + (b & 1)) & mask);
+                if (R >= 2) g |= (size_t)((u[1] + ((b >> 1) & 1)) & mask) << m.shift;
+                if (R == 3) g |= (size_t)((u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
                 if (v) atomicAdd(acc + cb + g, (unsigned long long)v);
             }
         }
@@ -1074,15 +1030,15 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     // divisions in the loop)
     const int E0 = org[3], E1 = org[4], E2 = org[5];
     const int ecells = E0 * E1 * E2;
-    int l0 = tid % E0, l1 = (tid / E0) % E1, l2 = tid / (E0 * E1);
+    int l0 = (int)threadIdx.x % E0, l1 = ((int)threadIdx.x / E0) % E1, l2 = (int)threadIdx.x / (E0 * E1);
     const int s0 = THREADS % E0, s1 = (THREADS / E0) % E1, s2 = THREADS / (E0 * E1);
-    for (int c = tid; c < ecells; c += THREADS) {
+    for (int c = threadIdx.x; c < ecells; c += THREADS) {
         const int wc = (l2 * W1 + l1) * W0 + l0;
         uint32_t a = lag_sh[wc], b = lag_sh[cells + wc];
         if (a | b) {
-            size_t g = (size_t)((b0 + o0 + l0) & mask);
-            if (R >= 2) g |= (size_t)((b1 + o1 + l1) & mask) << m.shift;
-            if (R == 3) g |= (size_t)((b2 + o2 + l2) & mask) << (2 * m.shift);
+            size_t g = (size_t)((o0 + l0) & mask);
+            if (R >= 2) g |= (size_t)((o1 + l1) & mask) << m.shift;
+            if (R == 3) g |= (size_t)((o2 + l2) & mask) << (2 * m.shift);
             atomicAdd(acc + cb + g, ((unsigned long long)b << 32) | a);
         }
         l0 += s0;
