@@ -224,6 +224,21 @@ def algorithmic_bytes(kernel, Np, Nc, fp64):
     return None
 
 
+def dram_traffic(kernel, workload):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu
+    summary (profiles/dram_traffic.txt), or None when it holds no such line."""
+    try:
+        for line in open(ROOT / "profiles" / "dram_traffic.txt"):
+            if line.startswith("#"):
+                continue
+            kv = dict(x.split("=", 1) for x in line.split() if "=" in x)
+            if kv.get("kernel") == kernel and kv.get("workload") == workload:
+                return float(kv["traffic_bytes"])
+    except OSError:
+        pass
+    return None
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -283,7 +298,8 @@ def run_ours(args):
     dom_ms = prof[dom][1] / prof[dom][0]
     ab = algorithmic_bytes(dom, Np, Nc, False)
     roof = {"kernel": dom, "bound": "hbm", "achieved": ab / (dom_ms * 1e-3) / 1e9, "peak": hbm,
-            "unit": "GB/s", "peak_source": hbm_src, "traffic": None,
+            "unit": "GB/s", "peak_source": hbm_src, "traffic": dram_traffic(dom, workload_name(mbits, f)),
+            "traffic_source": "profiles/dram_traffic.txt (ncu dram__bytes_read+write, per launch)",
             "algorithmic_bytes_per_launch": ab, "ms_per_launch": dom_ms}
     roof["frac"] = roof["achieved"] / hbm
     # the two rows the target names, each with every kernel it needs per step:

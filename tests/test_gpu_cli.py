@@ -1,0 +1,87 @@
+"""The drop-in CLI (`conan ic`, `conan run`) against the files the reference's
+own binary wrote for the same command lines (tests/golden/<case>.npz, made by
+tests/golden/make_golden.py from the unmodified reference).
+
+FP64 (`--precision fp64`): fields to 1e-11 and trajectories to 1e-9 of the
+field / box scale (cuFFT versus the reference's FFT rounding). The default FP32
+run: particle positions within a small fraction of a force cell.
+"""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = Path(__file__).resolve().parent.parent
+EXE = ROOT / "conan_b200" / "bin" / "conan"
+GOLD = ROOT / "tests" / "golden"
+CASES = ["c1s", "c2s", "c3s", "c4s"]
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _run(args, cwd):
+    r = subprocess.run([str(EXE), *args], cwd=cwd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+def _header_dict(lines):
+    return dict(str(l).split("=", 1) for l in lines)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_ic_and_fp64_run_reproduce_the_reference_files(gpu, tmp_path, name):
+    from conan_b200.conanfile import ConanFile
+    g = np.load(GOLD / f"{name}.npz")
+    _run(["ic", "-i", name, *str(g["ic_args"]).split()], tmp_path)
+    ic = ConanFile.read(str(tmp_path / f"{name}.density.init.conan"))
+    for rec in ("density", "potential", "displacement"):
+        if rec in g.files:
+            assert _rel(ic.records[rec], g[rec]) < 1e-11, rec
+    ref_hdr = _header_dict(g["ic_header"])
+    for k, v in ref_hdr.items():
+        assert ic.header.get(k) == v, (k, ic.header.get(k), v)
+
+    _run(["run", "-i", name, *str(g["run_args"]).split(), "--precision", "fp64"], tmp_path)
+    snaps = sorted(k[3:] for k in g.files if k.startswith("pos"))
+    assert snaps
+    L = float(ref_hdr["size"])
+    for k in snaps:
+        c = ConanFile.read(str(tmp_path / f"{name}.pos.{k}.conan"))
+        assert np.max(np.abs(c.records["pos"] - g[f"pos{k}"])) < 1e-9 * L, k
+        assert _rel(c.records["mom"], g[f"mom{k}"]) < 1e-8, k
+        for hk, hv in _header_dict(g[f"hdr{k}"]).items():
+            assert c.header.get(hk) == hv, (k, hk, c.header.get(hk), hv)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_default_fp32_run_tracks_the_reference(gpu, tmp_path, name):
+    from conan_b200.conanfile import ConanFile
+    g = np.load(GOLD / f"{name}.npz")
+    ic_file = tmp_path / f"{name}.density.init.conan"
+    _run(["ic", "-i", name, *str(g["ic_args"]).split()], tmp_path)
+    assert ic_file.exists()
+    _run(["run", "-i", name, *str(g["run_args"]).split()], tmp_path)
+    hdr = _header_dict(g["ic_header"])
+    run_args = str(g["run_args"]).split()
+    f = int(run_args[run_args.index("-f") + 1]) if "-f" in run_args else 2  # the reference's default f
+    cell = float(hdr["size"]) / (int(hdr["N"]) * f)
+    for k in sorted(k[3:] for k in g.files if k.startswith("pos")):
+        c = ConanFile.read(str(tmp_path / f"{name}.pos.{k}.conan"))
+        err = np.abs(c.records["pos"] - g[f"pos{k}"]) / cell
+        print(f"{name} snapshot {k}: FP32 position error rms {np.sqrt(np.mean(err ** 2)):.2e}, "
+              f"max {err.max():.2e} cells")
+        assert np.sqrt(np.mean(err ** 2)) < 1e-3 and err.max() < 5e-2
+
+
+def test_errors_follow_the_reference(gpu, tmp_path):
+    r = subprocess.run([str(EXE), "run", "-i", "missing"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode != 0 and "[error]" in (r.stdout + r.stderr)
+    r = subprocess.run([str(EXE), "nosuchcommand"], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert r.returncode != 0
