@@ -60,17 +60,49 @@ def workload_name(mbits, f):
 
 # ------------------------------------------------------------------ clocks --
 class Clocks:
-    """Samples nvidia-smi every 200 ms while the timed region runs."""
+    """Samples the SM clock and the clock-event (throttle) reasons while the
+    timed region runs: NVML read-only queries every 10 ms from a thread, or
+    nvidia-smi every 200 ms when NVML is unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.p = None
+        self.samples = []  # (sm_mhz, max_mhz, set of reasons)
+        self.thread = None
+
+    def _nvml_loop(self, nv, h):
+        import time as _t
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), {n for n, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            _t.sleep(0.01)
 
     def __enter__(self):
+        self.stop = False
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
@@ -80,7 +112,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        self.stop = True
+        if self.thread is not None:
+            self.thread.join(timeout=2)
         if self.p:
             self.p.terminate()
             try:
@@ -88,25 +122,23 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.p.kill()
                 out, _ = self.p.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            for l in out.splitlines():
+                f = [x.strip() for x in l.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.samples.append((float(f[1]), float(f[2]),
+                                         {n for n, v in zip(self.NAMES, f[5:9]) if v.lower().startswith("active")}))
+                except ValueError:
+                    continue
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
-            f = [x.strip() for x in l.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
+        sm = [x[0] for x in self.samples]
+        mx = self.samples[-1][1] if self.samples else None
+        reasons = set().union(*[x[2] for x in self.samples]) if self.samples else set()
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml 10 ms" if self.thread is not None else "nvidia-smi 200 ms"}
 
 
 # ------------------------------------------------------------ distributed --

@@ -75,6 +75,7 @@ struct Mesh {
     int cshift;  // R * shift: log2 of the cells of one member
     size_t mspec;  // nh * n^(R-1): spectrum values of one member
     int batch;
+    double inv_nh;  // 1 / nh, for the quotient of half-spectrum indices
 };
 
 inline Mesh make_mesh(int R, int n, int batch = 1) {
@@ -89,6 +90,7 @@ inline Mesh make_mesh(int R, int n, int batch = 1) {
     m.mspec = (size_t)m.nh;
     for (int i = 1; i < R; ++i) m.mspec *= (size_t)n;
     m.spec = m.mspec * (size_t)batch;
+    m.inv_nh = 1.0 / (double)m.nh;
     return m;
 }
 
@@ -102,9 +104,19 @@ __host__ __device__ inline int wave_index(int i, int n) { return i > n / 2 ? i -
 // Squared integer wave-vector length of half-spectrum element e (of any
 // member of the batch).
 __device__ inline long long spec_k2(size_t e, const Mesh &m, int *kv) {
-    if (m.batch > 1) e %= m.mspec;
-    int kx = (int)(e % (size_t)m.nh);
-    size_t rest = e / (size_t)m.nh;
+    // row = e / nh from the double reciprocal (exact after one correction:
+    // e < 2^53); the row's low (R-1) shift bits are the member's y, z
+    // indices, the bits above them the member (ignored)
+    size_t rest = (size_t)((double)e * m.inv_nh);
+    long long kr = (long long)e - (long long)rest * m.nh;
+    if (kr < 0) {
+        --rest;
+        kr += m.nh;
+    } else if (kr >= m.nh) {
+        ++rest;
+        kr -= m.nh;
+    }
+    int kx = (int)kr;
     long long s = (long long)kx * kx;
     kv[0] = kx;
     for (int a = 1; a < m.R; ++a) {

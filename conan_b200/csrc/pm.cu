@@ -375,10 +375,23 @@ template <typename T, int R> struct PM : PMBase {
             }
         }
         CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec, mesh)));
-        if (prm.gradient == CONAN_GRAD_FD4)
-            CONAN_TIMED(prof, "fd_grad", st,
-                        (k_fd_grad<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(mesh, grad, mf)));
+        if (prm.gradient == CONAN_GRAD_FD4) CONAN_TRY(fd_gradient(mesh, grad));
         mesh_holds = 2;
+        return CONAN_OK;
+    }
+
+    // Packed FD4 gradient mesh of phi (four cells per thread in FP32).
+    int fd_gradient(const T *phi, G4<T> *g) {
+        if constexpr (sizeof(T) == 4) {
+            if (mf.n >= 4) {
+                const size_t nt = mf.cells / 4;
+                CONAN_TIMED(prof, "fd_grad", st,
+                            (k_fd_grad4<R><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(phi, g, mf)));
+                return CONAN_OK;
+            }
+        }
+        CONAN_TIMED(prof, "fd_grad", st,
+                    (k_fd_grad<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(phi, g, mf)));
         return CONAN_OK;
     }
 
