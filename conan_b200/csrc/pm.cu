@@ -380,13 +380,12 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
-    // Packed FD4 gradient mesh of phi (four cells per thread in FP32).
+    // Packed FD4 gradient mesh of phi (x neighbours by warp shuffles in FP32).
     int fd_gradient(const T *phi, G4<T> *g) {
         if constexpr (sizeof(T) == 4) {
-            if (mf.n >= 4) {
-                const size_t nt = mf.cells / 4;
+            if (mf.n >= 32 && mf.cells % 256 == 0) {
                 CONAN_TIMED(prof, "fd_grad", st,
-                            (k_fd_grad4<R><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(phi, g, mf)));
+                            (k_fd_grad_w<R><<<(unsigned)(mf.cells / 256), 256, 0, st>>>(phi, g, mf)));
                 return CONAN_OK;
             }
         }
