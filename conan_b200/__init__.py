@@ -2,7 +2,7 @@
 
 The compute path is libconan_pm.so (CUDA sm_100a, C ABI in include/conan_pm.h);
 this package is its Python mirror. Importing it loads the library and fails
-loudly if the library has not been built (``python -m conan_b200.build``).
+loudly if the library has not been built (``python conan_b200/build.py``).
 """
 from . import _lib
 from ._lib import ConanError

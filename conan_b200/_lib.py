@@ -1,6 +1,6 @@
 """ctypes binding of libconan_pm.so (declarations mirror include/conan_pm.h).
 
-The library must have been built in-tree (``python -m conan_b200.build``);
+The library must have been built in-tree (``python conan_b200/build.py``);
 importing this module fails loudly when it is missing -- there is no CPU
 fallback for any entry point.
 """
@@ -113,7 +113,7 @@ def lib():
     global _lib
     if _lib is None:
         if not LIB_PATH.exists():
-            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m conan_b200.build`")
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python conan_b200/build.py`")
         L = C.CDLL(str(LIB_PATH))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name, None)

@@ -1,7 +1,8 @@
 """Builds the native parts of conan_b200 in-tree.
 
-    python -m conan_b200.build          # library + CLI
-    python -m conan_b200.build --clean
+    python conan_b200/build.py          # library + CLI (the package itself
+                                        # cannot be imported before this)
+    python conan_b200/build.py --clean
 
 Products (git-ignored, shipped with the tree):
     conan_b200/lib/libconan_pm.so   CUDA sm_100a kernels + the C ABI of include/conan_pm.h
