@@ -719,43 +719,6 @@ __global__ void __launch_bounds__(256) k_fd_grad(const T *__restrict__ phi, G4<T
     G[c] = G4<T>{g[0], g[1], g[2], T(0)};
 }
 
-// FP32 FD4 gradient, one cell per thread with a warp on 32 consecutive
-// cells of a row (n >= 32): the x neighbours come from warp shuffles (the
-// two lanes at each end of the warp load theirs), the y and z neighbours
-// from coalesced loads of the neighbouring rows, and the packed gradients
-// leave as coalesced 16-byte stores. Same stencil arithmetic as k_fd_grad.
-template <int R>
-__global__ void __launch_bounds__(256) k_fd_grad_w(const float *__restrict__ phi, G4<float> *__restrict__ G, Mesh m) {
-    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // m.cells is a multiple of 32
-    const uint32_t mask = m.n - 1;
-    const float c12 = 1.0f / 12.0f, c23 = 2.0f / 3.0f;
-    const int lane = threadIdx.x & 31;
-    const uint32_t x = (uint32_t)c & mask;
-    const size_t row = c - x;
-    const float v = __ldg(phi + c);
-    float m1 = __shfl_up_sync(FULL, v, 1), m2 = __shfl_up_sync(FULL, v, 2);
-    float p1 = __shfl_down_sync(FULL, v, 1), p2 = __shfl_down_sync(FULL, v, 2);
-    if (lane < 2) {
-        m2 = __ldg(phi + row + ((x - 2) & mask));
-        if (lane == 0) m1 = __ldg(phi + row + ((x - 1) & mask));
-    }
-    if (lane >= 30) {
-        p2 = __ldg(phi + row + ((x + 2) & mask));
-        if (lane == 31) p1 = __ldg(phi + row + ((x + 1) & mask));
-    }
-    float g[3];
-    g[0] = (m2 - p2) * c12 + (p1 - m1) * c23;
-#pragma unroll
-    for (int k = 1; k < R; ++k) {
-        const int sh = k * m.shift;
-        const uint32_t ck = (uint32_t)(c >> sh) & mask;
-        const size_t rest = c & ~((size_t)mask << sh);
-        auto at = [&](int o) { return __ldg(phi + (rest | ((size_t)((ck + o) & mask) << sh))); };
-        g[k] = (at(-2) - at(2)) * c12 + (at(1) - at(-1)) * c23;
-    }
-    reinterpret_cast<float4 *>(G)[c] = make_float4(g[0], R > 1 ? g[1] : 0.0f, R > 2 ? g[2] : 0.0f, 0.0f);
-}
-
 // CIC-interpolated force of particle i: sum over corners of weight times
 // the node gradient (packed FD4 mesh G, or the spectral gradient meshes g[k]).
 template <typename T, int R, bool SPECTRAL>
