@@ -911,9 +911,9 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
         if constexpr (FUSED) {
             float p[3];
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                d[k] = P.d[k][i];
-                p[k] = P.p[k][i];
+            for (int k = 0; k < R; ++k) {  // read once: evict-first, L1 stays for the gradients
+                d[k] = __ldcs(P.d[k] + i);
+                p[k] = __ldcs(P.p[k] + i);
             }
             if (gc.kick) {
                 float F[3];
