@@ -294,6 +294,61 @@ void oracle_md_cic(int R, int N, double L, const double *X, size_t n, double m, 
     }
 }
 
+/* The `cic` tool's density, cic_run<R> (src/cic/cic.hh:49-81): X holds the
+ * N^R absolute positions of a snapshot (AoS); out receives the Nf^R mesh,
+ * Nf = f N. s = 1: md_cic with unit mass. s > 1: the displacement X - G is
+ * interpolated linearly (LinearInterpolation, src/run/numeric.hh:6-45, on the
+ * mass grid) at the points of an (N s)^R grid (grid_space, src/base/box.hh:
+ * 11-24) and those points are deposited with mass (s N / Nf)^-R. */
+void oracle_cic(int R, int N, double L, int f, int s, const double *X, double *out) {
+    const int Nf = N * f;
+    const size_t np = ipow(N, R);
+    if (s == 1) {
+        oracle_md_cic(R, Nf, L, X, np, 1.0, out);
+        return;
+    }
+    const double res_m = L / N;
+    std::vector<double> D(np * R);
+    for (size_t i = 0; i < np; ++i) {
+        size_t r = i;
+        for (int k = 0; k < R; ++k) {
+            D[i * R + k] = X[i * R + k] - (double)(r % N) * (L / N);
+            r /= N;
+        }
+    }
+    const int Ns = N * s;
+    const size_t nsub = ipow(Ns, R);
+    std::vector<double> Y(nsub * R);
+    for (size_t j = 0; j < nsub; ++j) {
+        double y[8], x[8], A[2][8];
+        int origin[8];
+        size_t r = j;
+        for (int k = 0; k < R; ++k) {
+            y[k] = (double)(r % Ns) * (L / Ns);
+            r /= Ns;
+            x[k] = y[k] / res_m;
+            origin[k] = (int)x[k];
+            A[1][k] = x[k] - origin[k];
+            A[0][k] = 1 - A[1][k];
+        }
+        double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < (1 << R); ++b) {
+            double z = 1;
+            int c[8];
+            for (int k = 0; k < R; ++k) {
+                int bk = (b >> k) & 1;
+                z *= A[bk][k];
+                c[k] = origin[k] + bk;
+            }
+            size_t id = box_idx(c, R, N);
+            for (int k = 0; k < R; ++k) v[k] += D[id * R + k] * z;
+        }
+        for (int k = 0; k < R; ++k) Y[j * R + k] = y[k] + v[k];
+    }
+    const double a = std::pow(double(s * N) / double(Nf), -float(R));
+    oracle_md_cic(R, Nf, L, Y.data(), nsub, a, out);
+}
+
 /* Poisson solve on the force mesh: the FFT part of Gravity::kick,
  * src/run/nbody.hh:103-110. `delta` holds the deposit (mean 1) on entry and
  * phi = G/a * IFFT(-FFT(delta-1)/k^2)/size on return. */

@@ -92,6 +92,14 @@ def md_cic(dim, N, L, X, m=1.0) -> np.ndarray:
     return out
 
 
+def cic(dim, N, L, f, s, X) -> np.ndarray:
+    """The `cic` tool's density of a snapshot (cic_run, src/cic/cic.hh:49-81)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    out = np.empty((N * f) ** dim)
+    lib().oracle_cic(dim, N, _d(L), f, s, P(X), P(out))
+    return out
+
+
 def poisson(dim, N, L, G, a, delta_plus_one) -> np.ndarray:
     out = np.array(delta_plus_one, dtype=np.float64, copy=True)
     lib().oracle_poisson(dim, N, _d(L), _d(G), _d(a), P(out))

@@ -1,7 +1,8 @@
 """Generates the golden fixtures in this directory from the UNMODIFIED reference.
 
 Runs the reference's own `conan` binary (oracle/_ref/conan_ref, compiled from
-the reference sources by oracle/Makefile) through its public CLI, and the
+the reference sources by oracle/Makefile) through its public CLI (ic, run,
+cic), and the
 reference's own md_cic / LinearInterpolation<Gradient> templates through
 oracle/_ref/libconan_ref.so, on small seeded cases. Needs the reference tree
 (only in the build container); the fixtures it writes are committed.
@@ -37,6 +38,9 @@ CASES = {
             "-f 2 -c -a0 0.1 -da 0.05 -n 10"),
 }
 
+# (f, sub-sample) of the `cic` runs on every snapshot
+CIC_CASES = [(2, 1), (1, 2), (2, 2)]
+
 
 def run_cli(name, ic_args, run_args, work):
     exe = str(REF / "conan_ref")
@@ -56,6 +60,13 @@ def run_cli(name, ic_args, run_args, work):
         out[f"apos{k}"] = np.float64(c.header["a-pos"])
         out[f"amom{k}"] = np.float64(c.header["a-mom"])
         out[f"hdr{k}"] = np.array(sorted(f"{a}={b}" for a, b in c.header.items()))
+        # the `cic` tool on this snapshot (src/cic/main.cc): Eulerian factor f, sub-sampling s
+        for f, sub in CIC_CASES:
+            subprocess.run([exe, "cic", "-i", name, "-m", k, "-f", str(f), "-s", str(sub)], cwd=work, check=True,
+                           stdout=subprocess.DEVNULL)
+            r = ConanFile.read(str(Path(work) / f"{name}.rho.{k}.conan"))
+            out[f"rho{k}_f{f}_s{sub}"] = r.records["density"]
+            out[f"rhohdr{k}_f{f}_s{sub}"] = np.array(sorted(f"{a}={b}" for a, b in r.header.items()))
     return out, snaps
 
 

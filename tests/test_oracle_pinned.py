@@ -81,6 +81,20 @@ def test_oracle_run_matches_reference_snapshots(oracle, name, f, cosmo):
         assert abs(float(g[f"apos{snap}"]) - a) < 1e-4  # header keeps 6 significant digits
 
 
+@pytest.mark.parametrize("name", ["c1s", "c2s", "c3s", "c4s"])
+def test_oracle_cic_matches_reference_cic_tool(oracle, name):
+    """The `cic` tool of the reference (plain and sub-sampled) on its own snapshots."""
+    g = load_golden(name)
+    _, dim, mbits, L = _ic(g)
+    N = 1 << mbits
+    keys = [k for k in g if k.startswith("rho") and not k.startswith("rhohdr")]
+    assert keys
+    for k in keys:
+        snap, f, s = k[3:].split("_")
+        rho = oracle.cic(dim, N, L, int(f[1:]), int(s[1:]), g[f"pos{snap}"])
+        assert np.max(np.abs(rho - g[k])) <= 1e-12 * np.max(np.abs(g[k])), k
+
+
 @pytest.mark.parametrize("dim,N,L", [(2, 16, 10.0), (3, 8, 5.0), (1, 32, 7.0)])
 def test_oracle_kernels_match_reference_templates(oracle, dim, N, L):
     g = load_golden("kernels")
