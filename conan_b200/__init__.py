@@ -13,6 +13,7 @@ from .pm import (  # noqa: E402
     Cosmology,
     Gravity,
     LeapFrog,
+    cic,
     compute_displacement,
     compute_potential,
     generate_random_field,
@@ -22,6 +23,6 @@ from .pm import (  # noqa: E402
 from .conanfile import ConanFile  # noqa: E402
 
 __all__ = [
-    "ConanError", "ConanFile", "Cosmology", "Gravity", "LeapFrog", "compute_displacement",
+    "ConanError", "ConanFile", "Cosmology", "Gravity", "LeapFrog", "cic", "compute_displacement",
     "compute_potential", "generate_random_field", "ic_params", "white_noise",
 ]

@@ -33,6 +33,11 @@ class PMParams(C.Structure):
                 ("device", C.c_int)]
 
 
+class CicParams(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n_mass", C.c_int), ("f", C.c_int), ("size", C.c_double),
+                ("sub_sample", C.c_int), ("device", C.c_int)]
+
+
 class DiffParams(C.Structure):
     _fields_ = [("ic", ICParams), ("pm", PMParams), ("a0", C.c_double), ("da", C.c_double),
                 ("n", C.c_uint), ("checkpoint_every", C.c_uint)]
@@ -59,6 +64,7 @@ SIGNATURES = {
     "conan_ic_generate": (C.c_int, [C.POINTER(ICParams), _dp, _dp]),
     "conan_ic_potential": (C.c_int, [C.POINTER(ICParams), _dp]),
     "conan_ic_displacement": (C.c_int, [C.POINTER(ICParams), _dp, _dp]),
+    "conan_cic": (C.c_int, [C.POINTER(CicParams), _dp, _dp]),
     "conan_pm_create": (C.c_void_p, [C.POINTER(PMParams)]),
     "conan_pm_destroy": (None, [C.c_void_p]),
     "conan_pm_init": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double]),

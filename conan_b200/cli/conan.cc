@@ -1,12 +1,16 @@
-// conan -- host CLI with the reference's `ic` and `run` commands on the GPU.
+// conan -- host CLI with the reference's `ic`, `run` and `cic` commands on the
+// GPU.
 //
 // Drop-in for the reference binary's sub-commands (src/base/main.cc:95-119):
-// the same option tables (src/ic/main.cc:15-65, src/run/main.cc:20-61), the
-// same header/history merge (src/base/header.cc:22-28, src/base/history.cc),
-// the same file contracts: `ic` writes <id>.density.init.conan with records
-// density [, potential] [, displacement]; `run` reads its potential record and
-// writes <id>.pos.<k>.conan every 10 steps (or IFRIT .bin / ASCII .txt),
-// src/run/nbody.hh:135-218. The numerics run in libconan_pm.so.
+// the same option tables (src/ic/main.cc:15-65, src/run/main.cc:20-61,
+// src/cic/main.cc:17-32), the same header/history merge (src/base/header.cc:
+// 22-28, src/base/history.cc), the same file contracts: `ic` writes
+// <id>.density.init.conan with records density [, potential] [,
+// displacement]; `run` reads its potential record and writes
+// <id>.pos.<k>.conan every 10 steps (or IFRIT .bin / ASCII .txt),
+// src/run/nbody.hh:135-218; `cic` reads <id>.pos.<m>.conan and writes
+// <id>.rho.<m>.conan (src/cic/main.cc:43-79). The numerics run in
+// libconan_pm.so.
 //
 // Options that only this build has (precision, noise source, gradient,
 // device, periodic gather) are marked local: they are parsed like the others
@@ -515,11 +519,72 @@ void cmd_run(int argc, char **argv) {
     if (rc != CONAN_OK) throw Fail(msg);
 }
 
+// ---------------------------------------------------------------- cic ----
+
+// The `cic` tool (src/cic/main.cc:11-82): density of snapshot <id>.pos.<m>
+// on the (f N)^dim mesh, written as <id>.rho.<m>.conan.
+void cmd_cic(int argc, char **argv) {
+    Argv C;
+    C.opts = {
+        {0, "h", "help", "false", "print help on the use of this program."},
+        {Option::VALUED | Option::CHECK, "i", "id", date_string(), "identifier for filenames."},
+        {Option::VALUED | Option::CHECK, "f", "f", "2",
+         "fractional Eulerian resolution. The default makes the Eulerian grid twice the size of the mass grid."},
+        {Option::VALUED | Option::CHECK, "m", "m", "5", "snap-shot"},
+        {Option::VALUED | Option::CHECK, "s", "sub-sample", "1", "subsample the grid and interpolate the position."},
+        {Option::VALUED | Option::CHECK | Option::LOCAL, "", "device", "0", "CUDA device."},
+    };
+    C.parse(argc, argv);
+    if (C.flag("help")) {
+        std::cout << "Cosmic workset Conan (B200 build).\n\n";
+        C.print(std::cout);
+        exit(0);
+    }
+    unsigned m = C.get<unsigned>("m");
+    std::ifstream fi(fmt(C["id"], ".pos.", m, ".conan"), std::ios::binary);
+    if (!fi) throw Fail("Could not read from file");
+    Header H;
+    H.from_file(fi);
+    H << C;
+    History I;
+    I.from_file(fi);
+    I.update(C.command_line);
+    unsigned f = H.get<unsigned>("f"), N = H.get<unsigned>("N");
+    double L = H.get<double>("L");
+    unsigned s = H.get<unsigned>("sub-sample");
+    if (H.count("dim") == 0) H["dim"] = "3";
+    int dim = H.get<int>("dim");
+    std::vector<double> X = load_record(fi, "pos");
+    fi.close();
+    size_t np = 1;
+    for (int k = 0; k < dim; ++k) np *= N;
+    if (X.size() != np * (size_t)dim) throw Fail("pos record has the wrong size");
+
+    conan_cic_params p{};
+    p.dim = dim;
+    p.n_mass = (int)N;
+    p.f = (int)f;
+    p.size = L;
+    p.sub_sample = (int)s;
+    p.device = C.get<int>("device");
+    size_t nc = 1;
+    for (int k = 0; k < dim; ++k) nc *= (size_t)N * f;
+    std::vector<double> rho(nc);
+    check(conan_cic(&p, X.data(), rho.data()));
+
+    std::ofstream fo(fmt(C["id"], ".rho.", m, ".conan"), std::ios::binary);
+    if (!fo) throw Fail("could not write the density file");
+    H["N"] = fmt(N * f);
+    H.to_file(fo);
+    I.to_file(fo);
+    save_record(fo, "density", "float64", rho.data(), rho.size() * sizeof(double));
+}
+
 void usage(const std::string &cmd) {
     std::cout << "Conan - cosmological tool chain - NBody code (B200 build).\n\n"
                  "This is a very basic N-body code, using Particle-Mesh method.\n\n"
                  "usage: "
-              << cmd << " [command] [args]\nwhere [command] is one of: ic, run\nto get help on a command: " << cmd
+              << cmd << " [command] [args]\nwhere [command] is one of: ic, run, cic\nto get help on a command: " << cmd
               << " [command] --help\n";
 }
 
@@ -530,7 +595,7 @@ int main(int argc, char **argv) {
         usage(argv[0]);
         return 0;
     }
-    std::map<std::string, std::function<void(int, char **)>> commands = {{"ic", cmd_ic}, {"run", cmd_run}};
+    std::map<std::string, std::function<void(int, char **)>> commands = {{"ic", cmd_ic}, {"run", cmd_run}, {"cic", cmd_cic}};
     std::string command(argv[1]);
     try {
         auto it = commands.find(command);

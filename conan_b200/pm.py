@@ -97,6 +97,21 @@ def compute_displacement(H: Dict, potential: np.ndarray, precision: str = "fp64"
     return out
 
 
+def cic(X: np.ndarray, dim: int, n_mass: int, L_box: float, f: int = 2, sub_sample: int = 1,
+        device: int = 0) -> np.ndarray:
+    """The `cic` tool, cic_run<R> (src/cic/cic.hh:49-81): density of a
+    snapshot's positions X (n_mass^dim x dim, absolute) on the (f n_mass)^dim
+    mesh, optionally from a sub_sample-times finer interpolated grid."""
+    p = L.CicParams()
+    p.dim, p.n_mass, p.f, p.size, p.sub_sample, p.device = dim, n_mass, f, float(L_box), sub_sample, device
+    x = np.ascontiguousarray(X, dtype=np.float64)
+    if x.size != n_mass ** dim * dim:
+        raise ValueError(f"expected {n_mass ** dim} x {dim} positions, got {x.shape}")
+    out = np.empty((n_mass * f) ** dim)
+    L.check(L.lib().conan_cic(C.byref(p), L.ptr(x), L.ptr(out)))
+    return out
+
+
 class Cosmology:
     """src/run/cosmology.hh:6-28."""
 

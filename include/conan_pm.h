@@ -94,6 +94,28 @@ int conan_ic_potential(const conan_ic_params *p, double *inout);
  * without the file write: psi_out receives N^dim x dim doubles (AoS). */
 int conan_ic_displacement(const conan_ic_params *p, const double *potential, double *psi_out);
 
+/* ----------------------------------------------------------------- cic -- */
+
+/* Options of the `cic` tool, src/cic/main.cc:17-32, with the snapshot's box. */
+typedef struct {
+    int dim;         /* 1..3 */
+    int n_mass;      /* particles per side N of the snapshot (power of two) */
+    int f;           /* --f, Eulerian mesh = f * N per side (power of two) */
+    double size;     /* box size L */
+    int sub_sample;  /* --sub-sample s >= 1 (power of two) */
+    int device;      /* CUDA device ordinal */
+} conan_cic_params;
+
+/* cic_run<R>, src/cic/cic.hh:49-81: the density of a snapshot on the (f N)^dim
+ * mesh. X: N^dim absolute positions (AoS doubles, the snapshot's `pos`
+ * record). s = 1: CIC deposit of unit masses (md_cic_T, src/cic/cic.hh:8-47).
+ * s > 1: the displacement X - q is interpolated linearly on the mass grid at
+ * the points of an (s N)^dim grid, which are deposited with mass
+ * (s N / (f N))^-dim. rho_out: (f N)^dim doubles, the sum of the deposited
+ * masses per cell (no normalisation). FP64 positions and weights; integer
+ * accumulation (2^-40 units), so the result does not depend on the order. */
+int conan_cic(const conan_cic_params *p, const double *X, double *rho_out);
+
 /* ------------------------------------------------------------------ pm -- */
 
 /* Parameters of the `run` tool, src/run/main.cc:20-61,82-103, as the

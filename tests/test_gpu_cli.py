@@ -85,3 +85,25 @@ def test_errors_follow_the_reference(gpu, tmp_path):
     assert r.returncode != 0 and "[error]" in (r.stdout + r.stderr)
     r = subprocess.run([str(EXE), "nosuchcommand"], cwd=tmp_path, capture_output=True, text=True, timeout=120)
     assert r.returncode != 0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_cic_tool_reproduces_the_reference_files(gpu, tmp_path, name):
+    """`conan cic` (plain and sub-sampled) on the reference's own snapshots,
+    against the density files its own `cic` wrote for the same options."""
+    from conan_b200.conanfile import ConanFile
+    g = np.load(GOLD / f"{name}.npz")
+    keys = [k for k in g.files if k.startswith("rho") and not k.startswith("rhohdr")]
+    assert keys
+    for k in keys:
+        snap, f, s = k[3:].split("_")
+        hdr = _header_dict(g[f"hdr{snap}"])
+        c = ConanFile(header=hdr)
+        c.update_history("ran nbody")
+        c.add("pos", g[f"pos{snap}"])
+        c.add("mom", g[f"mom{snap}"])
+        c.write(str(tmp_path / f"{name}.pos.{snap}.conan"))
+        _run(["cic", "-i", name, "-m", snap, "-f", f[1:], "-s", s[1:]], tmp_path)
+        r = ConanFile.read(str(tmp_path / f"{name}.rho.{snap}.conan"))
+        assert _rel(r.records["density"], g[k]) < 1e-11, k
+        assert r.header == _header_dict(g[f"rhohdr{snap}_{f}_{s}"]), k

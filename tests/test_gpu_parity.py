@@ -260,3 +260,16 @@ def test_spectral_gradient_runs_and_is_close_to_fd4(gpu, conan, oracle):
     cell = L / Nm
     d = np.max(np.abs(out[0] - out[1])) / cell
     assert 0 < d < 0.05
+
+
+@pytest.mark.parametrize("dim,Nm,f,s", [(3, 16, 2, 1), (3, 16, 1, 2), (3, 8, 2, 4), (2, 32, 2, 2), (2, 64, 1, 1),
+                                        (1, 128, 2, 4), (3, 32, 1, 1)])
+def test_cic_tool_matches_oracle(gpu, conan, oracle, dim, Nm, f, s):
+    """conan_cic against the oracle's cic_run (positions anywhere, wrapped)."""
+    L = 30.0
+    X, _ = _particles(dim, Nm, f, L, 6.0, 11)
+    got = conan.cic(X, dim, Nm, L, f=f, sub_sample=s)
+    ref = oracle.cic(dim, Nm, L, f, s, X)
+    assert np.max(np.abs(got - ref)) <= 1e-11 * np.max(np.abs(ref))
+    assert abs(got.sum() - Nm ** dim) < 1e-6 * Nm ** dim  # mass conservation
+    assert np.array_equal(got, conan.cic(X, dim, Nm, L, f=f, sub_sample=s))  # order-independent sums
