@@ -271,5 +271,8 @@ def test_cic_tool_matches_oracle(gpu, conan, oracle, dim, Nm, f, s):
     got = conan.cic(X, dim, Nm, L, f=f, sub_sample=s)
     ref = oracle.cic(dim, Nm, L, f, s, X)
     assert np.max(np.abs(got - ref)) <= 1e-11 * np.max(np.abs(ref))
-    assert abs(got.sum() - Nm ** dim) < 1e-6 * Nm ** dim  # mass conservation
+    # total mass: N^dim unit masses, but (f N)^dim when sub-sampled, since
+    # the reference weights the (s N)^dim points by (s N / f N)^-dim
+    total = Nm ** dim if s == 1 else (Nm * f) ** dim
+    assert abs(got.sum() - total) < 1e-9 * total
     assert np.array_equal(got, conan.cic(X, dim, Nm, L, f=f, sub_sample=s))  # order-independent sums
