@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-cic", action="store_true")
     return ap.parse_args()
 
 
@@ -382,6 +383,27 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
     g.close()
 
+    # the cic tool on the final snapshot (host positions in, host density out)
+    cic = None
+    if rank == 0 and not args.no_cic:
+        from oracle import cpu as oracle
+        cic = {}
+        for s in (1, 2):
+            cb.cic(Xh, 3, n, L_BOX, f=1, sub_sample=s, device=dev)  # warm-up
+            t0 = time.perf_counter()
+            cb.cic(Xh, 3, n, L_BOX, f=1, sub_sample=s, device=dev)
+            dt = time.perf_counter() - t0
+            cic[f"s{s}"] = {"points_per_s": (n * s) ** 3 / dt, "seconds": dt}
+        m = 6  # CPU restatement on a 64^3 sample of the same box (one thread)
+        Xs = Xh.reshape(n, n, n, 3)[:: n >> m, :: n >> m, :: n >> m].reshape(-1, 3)
+        t0 = time.perf_counter()
+        oracle.cic(3, 1 << m, L_BOX, 1, 2, Xs)
+        dt = time.perf_counter() - t0
+        cic["cpu_port_s2"] = {"points_per_s": (2 << m) ** 3 / dt, "cores": 1,
+                              "sample": "64^3 particles (every 8th lattice point), s=2, f=1"}
+        cic["what"] = ("conan_cic on the final 512^3 FP32 snapshot, f=1 (512^3 mesh), s=1 and s=2 (1024^3 "
+                       "interpolated points); host positions in, host density out")
+
     adjoint = None
     if not args.no_adjoint and rank == 0:
         try:
@@ -443,6 +465,7 @@ def run_ours(args):
             "fp64_gpu": fp64,
             "adjoint": adjoint,
             "ensemble": ensemble,
+            "cic": cic,
             "e2e": {"value": world * Np * args.steps / e2e_s, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": phi.nbytes / args.steps,
                     "d2h_bytes_per_step": (Xh.nbytes + Ph.nbytes) / args.steps,
