@@ -78,7 +78,7 @@ def build(verbose: bool = False, extra_flags=()) -> Path:
     cli_src = sorted(CLI.glob("*.cc"))
     cli_hdr = list(CLI.glob("*.hh")) + list((ROOT / "include").glob("*.h"))
     if cli_src and _newer(EXE, [*cli_src, *cli_hdr, LIB]):
-        _run([CXX, "-std=c++17", "-O2", "-Wall", f"-I{ROOT / 'include'}", *map(str, cli_src),
+        _run([CXX, "-std=c++17", "-O2", "-Wall", "-pthread", f"-I{ROOT / 'include'}", *map(str, cli_src),
               "-o", str(EXE), f"-L{LIBDIR}", "-lconan_pm", "-Wl,-rpath,$ORIGIN/../lib"])
     return LIB
 

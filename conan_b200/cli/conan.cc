@@ -26,9 +26,11 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <memory>
 #include <random>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "conan_pm.h"
@@ -351,6 +353,16 @@ void cmd_ic(int argc, char **argv) {
 
 enum Format { FMT_ASCII, FMT_IFRIT, FMT_CONAN };
 
+// Snapshot writing overlaps the GPU: the callback copies the state to host
+// memory and hands it to a writer thread, then the run continues while the
+// file is written; the next snapshot (and the end of the run) waits for the
+// previous writer. At most two snapshots are held in host memory.
+struct Snapshot {
+    unsigned index;
+    double a, a_pos, a_mom;
+    std::vector<double> X, P;
+};
+
 struct RunCtx {
     std::string id;
     int dim;
@@ -358,29 +370,30 @@ struct RunCtx {
     double L;
     Format format;
     size_t np;
+    std::thread writer;
+    std::string writer_error;
+
+    void join() {
+        if (writer.joinable()) writer.join();
+        if (!writer_error.empty()) throw Fail(writer_error);
+    }
 };
 
-void save_snapshot(conan_pm *h, RunCtx &c, unsigned i, double a) {
-    std::cout << "|";
-    std::cout.flush();
-    std::vector<double> X(c.np * c.dim), P(c.np * c.dim);
-    check(conan_pm_get_state(h, X.data(), P.data()));
-    double a_pos = 0, a_mom = 0;
-    check(conan_pm_scale_factors(h, &a_pos, &a_mom));
+void write_snapshot(const RunCtx &c, const Snapshot &s) {
     const char *ext = c.format == FMT_ASCII ? ".txt" : c.format == FMT_IFRIT ? ".bin" : ".conan";
-    std::string fn = fmt(c.id, ".pos.", (i + 1) / 10, ext);
+    std::string fn = fmt(c.id, ".pos.", s.index, ext);
     std::ofstream fo(fn, std::ios::binary);
     if (!fo) throw Fail("could not open " + fn);
+    const std::vector<double> &X = s.X, &P = s.P;
     if (c.format == FMT_ASCII) {
         // X[i] " " P[i]/a with mVector's trailing-space printing.
         for (size_t j = 0; j < c.np; ++j) {
             for (int k = 0; k < c.dim; ++k) fo << X[j * c.dim + k] << " ";
             fo << " ";
-            for (int k = 0; k < c.dim; ++k) fo << P[j * c.dim + k] / a << " ";
+            for (int k = 0; k < c.dim; ++k) fo << P[j * c.dim + k] / s.a << " ";
             fo << "\n";
         }
     } else if (c.format == FMT_IFRIT) {
-        if (c.dim != 3) throw Fail("IFRIT files only support 3D");
         uint32_t N = (uint32_t)c.np;
         write_block_32(fo, &N, 4);
         float dims[6] = {0, 0, 0, (float)c.L, (float)c.L, (float)c.L};
@@ -398,8 +411,8 @@ void save_snapshot(conan_pm *h, RunCtx &c, unsigned i, double a) {
         H["N"] = fmt(c.N);
         H["L"] = fmt(c.L);
         H["dim"] = fmt(c.dim);
-        H["a-mom"] = fmt(a_mom);
-        H["a-pos"] = fmt(a_pos);
+        H["a-mom"] = fmt(s.a_mom);
+        H["a-pos"] = fmt(s.a_pos);
         History I;
         I.update("ran nbody");
         H.to_file(fo);
@@ -408,6 +421,28 @@ void save_snapshot(conan_pm *h, RunCtx &c, unsigned i, double a) {
         save_record(fo, "pos", dt, X.data(), X.size() * sizeof(double));
         save_record(fo, "mom", dt, P.data(), P.size() * sizeof(double));
     }
+    if (!fo) throw Fail("could not write " + fn);
+}
+
+void save_snapshot(conan_pm *h, RunCtx &c, unsigned i, double a) {
+    std::cout << "|";
+    std::cout.flush();
+    if (c.format == FMT_IFRIT && c.dim != 3) throw Fail("IFRIT files only support 3D");
+    auto s = std::make_shared<Snapshot>();
+    s->index = (i + 1) / 10;
+    s->a = a;
+    s->X.resize(c.np * c.dim);
+    s->P.resize(c.np * c.dim);
+    check(conan_pm_get_state(h, s->X.data(), s->P.data()));
+    check(conan_pm_scale_factors(h, &s->a_pos, &s->a_mom));
+    c.join();  // the previous snapshot's file is complete
+    c.writer = std::thread([&c, s] {
+        try {
+            write_snapshot(c, *s);
+        } catch (std::exception &e) {
+            c.writer_error = e.what();
+        }
+    });
 }
 
 struct CbData {
@@ -514,6 +549,12 @@ void cmd_run(int argc, char **argv) {
     check(conan_pm_set_callback_interval(h, 10));
     int rc = conan_pm_run(h, phi.data(), a0, da, n, step_cb, &cbd);
     std::string msg = rc == CONAN_OK ? "" : (cbd.error.empty() ? conan_last_error() : cbd.error);
+    try {
+        ctx.join();  // the last snapshot's file
+    } catch (std::exception &e) {
+        if (msg.empty()) msg = e.what();
+        rc = rc == CONAN_OK ? CONAN_ERR_IO : rc;
+    }
     conan_pm_destroy(h);
     std::cout << std::endl;
     if (rc != CONAN_OK) throw Fail(msg);

@@ -107,3 +107,20 @@ def test_cic_tool_reproduces_the_reference_files(gpu, tmp_path, name):
         r = ConanFile.read(str(tmp_path / f"{name}.rho.{snap}.conan"))
         assert _rel(r.records["density"], g[k]) < 1e-11, k
         assert r.header == _header_dict(g[f"rhohdr{snap}_{f}_{s}"]), k
+
+
+def test_ifrit_and_ascii_snapshots(gpu, tmp_path):
+    """The other two snapshot formats of the reference (src/run/nbody.hh:135-166)."""
+    g = np.load(GOLD / "c3s.npz")
+    _run(["ic", "-i", "c3s", *str(g["ic_args"]).split()], tmp_path)
+    _run(["run", "-i", "c3s", *str(g["run_args"]).split(), "--precision", "fp64", "--ascii"], tmp_path)
+    rows = np.loadtxt(tmp_path / "c3s.pos.1.txt")
+    assert rows.shape == (8 ** 3, 6)
+    assert np.max(np.abs(rows[:, :3] - g["pos1"])) < 1e-4 * 40  # printed with 6 significant digits
+    _run(["run", "-i", "c3s", *str(g["run_args"]).split(), "--precision", "fp64", "--ifrit"], tmp_path)
+    raw = (tmp_path / "c3s.pos.1.bin").read_bytes()
+    n = np.frombuffer(raw[4:8], dtype=np.uint32)[0]
+    assert n == 8 ** 3
+    off = 4 + 4 + 4 + (4 + 24 + 4)
+    x = np.frombuffer(raw[off + 4: off + 4 + 4 * n], dtype=np.float32)
+    assert np.allclose(x, g["pos1"][:, 0], rtol=1e-6, atol=1e-5)
