@@ -414,14 +414,13 @@ template <typename T, int R> struct Diff : DiffBase {
     int adjoint_poisson(double am) {
         cudaStream_t st = pm.st;
         const Mesh &mf = pm.mf;
-        unsigned gc = (unsigned)((mf.cells + 255) / 256), gs = (unsigned)((mf.spec + 255) / 256);
+        unsigned gc = (unsigned)((mf.cells + 255) / 256);
         k_neg_div<T, R, unsigned long long><<<gc, 256, 0, st>>>(U[0], U[1], U[2], S, rhobar, mf);
         CONAN_LAUNCHED();
         // per-member normalisation: 1 / (cells of one box)
         double gsc = -pm.G / (am * (double)((size_t)1 << mf.cshift)) * std::pow(prm.pm.size / (2 * M_PI), 2);
         CONAN_TRY(pm.fft.forward(rhobar, pm.spec));
-        k_green<T><<<gs, 256, 0, st>>>(pm.spec, mf, (T)gsc);
-        CONAN_LAUNCHED();
+        CONAN_TRY(pm.green(pm.spec, gsc));
         CONAN_TRY(pm.fft.inverse(pm.spec, rhobar));
         return CONAN_OK;
     }

@@ -362,12 +362,20 @@ template <typename T, int R> struct PM : PMBase {
     }
 
     // --- Poisson: mesh (delta) -> mesh (phi) [and gradient meshes] ------
+    // Green's function multiply of the half spectrum s (one CTA per row).
+    int green(CT *s, double gs) {
+        const unsigned rows = (unsigned)(mf.spec / (size_t)mf.nh);
+        const int threads = mf.nh >= 256 ? 256 : ((mf.nh + 31) / 32) * 32;
+        CONAN_TIMED(prof, "green", st, (k_green<T><<<rows, threads, 0, st>>>(s, mf, (T)gs)));
+        return CONAN_OK;
+    }
+
     int poisson(double a) {
         // per-member normalisation: 1 / (cells of one box)
         double gs = -G / (a * (double)((size_t)1 << mf.cshift)) * std::pow(prm.size / (2 * M_PI), 2);
         unsigned gb = (unsigned)((mf.spec + 255) / 256);
         CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
-        CONAN_TIMED(prof, "green", st, (k_green<T><<<gb, 256, 0, st>>>(spec, mf, (T)gs)));
+        CONAN_TRY(green(spec, gs));
         if (prm.gradient == CONAN_GRAD_SPECTRAL) {
             for (int k = 0; k < R; ++k) {
                 CONAN_TIMED(prof, "spec_deriv", st, (k_spec_deriv<T><<<gb, 256, 0, st>>>(spec, spec2, mf, k)));

@@ -622,17 +622,27 @@ __global__ void k_deposit_pull(const uint32_t *__restrict__ off,
 // Green's function multiply on the half spectrum: spec *= gs / |n|^2 with
 // gs = -G/(a N_c) (L/2pi)^2, DC = 0 (src/run/nbody.hh:105-110 with
 // Fourier::potential, src/base/fourier.hh:102-109).
+// One CTA per row of the half spectrum (n/2 + 1 elements along kx): the
+// row's ky, kz come from the block index by bit operations, so no element
+// index is ever divided.
 template <typename T>
-__global__ void k_green(typename Cplx<T>::type *__restrict__ spec, Mesh m, T gs) {
-    size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= m.spec) return;
-    int kv[3];
-    long long k2 = spec_k2(e, m, kv);
-    T g = k2 > 0 ? gs / (T)k2 : T(0);
-    auto z = spec[e];
-    z.x *= g;
-    z.y *= g;
-    spec[e] = z;
+__global__ void __launch_bounds__(256) k_green(typename Cplx<T>::type *__restrict__ spec, Mesh m, T gs) {
+    const size_t row = blockIdx.x;  // n^(R-1) rows per member, members back to back
+    long long kyz = 0;
+    for (int a = 1; a < m.R; ++a) {
+        const int ia = (int)((row >> ((a - 1) * m.shift)) & (size_t)(m.n - 1));
+        const int w = wave_index(ia, m.n);
+        kyz += (long long)w * w;
+    }
+    typename Cplx<T>::type *r = spec + row * (size_t)m.nh;
+    for (int kx = threadIdx.x; kx < m.nh; kx += blockDim.x) {
+        const long long k2 = (long long)kx * kx + kyz;
+        T g = k2 > 0 ? gs / (T)k2 : T(0);
+        auto z = r[kx];
+        z.x *= g;
+        z.y *= g;
+        r[kx] = z;
+    }
 }
 
 // Spectral derivative along `axis` in cell units: out = i (2 pi n_axis / n)
