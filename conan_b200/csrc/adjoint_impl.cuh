@@ -420,7 +420,7 @@ template <typename T, int R> struct Diff : DiffBase {
         // per-member normalisation: 1 / (cells of one box)
         double gsc = -pm.G / (am * (double)((size_t)1 << mf.cshift)) * std::pow(prm.pm.size / (2 * M_PI), 2);
         CONAN_TRY(pm.fft.forward(rhobar, pm.spec));
-        CONAN_TRY(pm.green(pm.spec, pm.spec, gsc));
+        CONAN_TRY(pm.green(pm.spec, gsc));
         CONAN_TRY(pm.fft.inverse(pm.spec, rhobar));
         return CONAN_OK;
     }

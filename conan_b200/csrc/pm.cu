@@ -142,8 +142,8 @@ template <typename T, int R> struct PM : PMBase {
         }
         CONAN_TRY(alloc(&mesh, mf.cells));
         CONAN_TRY(alloc(&spec, mf.spec));
-        CONAN_TRY(alloc(&spec2, mf.spec));  // Green output / spectral derivatives
         if (p.gradient == CONAN_GRAD_SPECTRAL) {
+            CONAN_TRY(alloc(&spec2, mf.spec));
             for (int k = 0; k < R; ++k) CONAN_TRY(alloc(&gm[k], mf.cells));
         } else {
             CONAN_TRY(alloc(&grad, mf.cells));
@@ -363,10 +363,10 @@ template <typename T, int R> struct PM : PMBase {
 
     // --- Poisson: mesh (delta) -> mesh (phi) [and gradient meshes] ------
     // Green's function multiply of the half spectrum s (one CTA per row).
-    int green(const CT *in, CT *out, double gs) {
+    int green(CT *s, double gs) {
         const unsigned rows = (unsigned)(mf.spec / (size_t)mf.nh);
         const int threads = mf.nh >= 256 ? 256 : ((mf.nh + 31) / 32) * 32;
-        CONAN_TIMED(prof, "green", st, (k_green<T><<<rows, threads, 0, st>>>(in, out, mf, (T)gs)));
+        CONAN_TIMED(prof, "green", st, (k_green<T><<<rows, threads, 0, st>>>(s, mf, (T)gs)));
         return CONAN_OK;
     }
 
@@ -375,17 +375,14 @@ template <typename T, int R> struct PM : PMBase {
         double gs = -G / (a * (double)((size_t)1 << mf.cshift)) * std::pow(prm.size / (2 * M_PI), 2);
         unsigned gb = (unsigned)((mf.spec + 255) / 256);
         CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
+        CONAN_TRY(green(spec, gs));
         if (prm.gradient == CONAN_GRAD_SPECTRAL) {
-            CONAN_TRY(green(spec, spec, gs));
             for (int k = 0; k < R; ++k) {
                 CONAN_TIMED(prof, "spec_deriv", st, (k_spec_deriv<T><<<gb, 256, 0, st>>>(spec, spec2, mf, k)));
                 CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec2, gm[k])));
             }
-            CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec, mesh)));
-        } else {
-            CONAN_TRY(green(spec, spec2, gs));  // out of place
-            CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec2, mesh)));
         }
+        CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft.inverse(spec, mesh)));
         if (prm.gradient == CONAN_GRAD_FD4) CONAN_TRY(fd_gradient(mesh, grad));
         mesh_holds = 2;
         return CONAN_OK;

@@ -624,11 +624,9 @@ __global__ void k_deposit_pull(const uint32_t *__restrict__ off,
 // Fourier::potential, src/base/fourier.hh:102-109).
 // One CTA per row of the half spectrum (n/2 + 1 elements along kx): the
 // row's ky, kz come from the block index by bit operations, so no element
-// index is ever divided. `out` may be `in`; a separate output streams faster
-// than the in-place update.
+// index is ever divided.
 template <typename T>
-__global__ void __launch_bounds__(256) k_green(const typename Cplx<T>::type *in, typename Cplx<T>::type *out,
-                                               Mesh m, T gs) {
+__global__ void __launch_bounds__(256) k_green(typename Cplx<T>::type *__restrict__ spec, Mesh m, T gs) {
     const size_t row = blockIdx.x;  // n^(R-1) rows per member, members back to back
     long long kyz = 0;
     for (int a = 1; a < m.R; ++a) {
@@ -636,15 +634,14 @@ __global__ void __launch_bounds__(256) k_green(const typename Cplx<T>::type *in,
         const int w = wave_index(ia, m.n);
         kyz += (long long)w * w;
     }
-    const typename Cplx<T>::type *r = in + row * (size_t)m.nh;
-    typename Cplx<T>::type *w = out + row * (size_t)m.nh;
+    typename Cplx<T>::type *r = spec + row * (size_t)m.nh;
     for (int kx = threadIdx.x; kx < m.nh; kx += blockDim.x) {
         const long long k2 = (long long)kx * kx + kyz;
         T g = k2 > 0 ? gs / (T)k2 : T(0);
         auto z = r[kx];
         z.x *= g;
         z.y *= g;
-        w[kx] = z;
+        r[kx] = z;
     }
 }
 
