@@ -2,6 +2,7 @@
 // kernels of libconan_pm.so.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the encoder is fetched from the driver at run time)
 #include <cuda_runtime.h>
 #include <cufft.h>
 

@@ -161,6 +161,7 @@ template <typename T, int R> struct PM : PMBase {
             CONAN_TRY(alloc(&lacc, mf.cells));
             CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st));
             dep_variant = DEP_LAG;
+            CONAN_TRY(tma_setup());
         }
         CONAN_TRY(fft.create(mf, sizeof(T) == 8, batch));
         CONAN_TRY(alloc((char **)&work, fft.work_bytes));
@@ -243,11 +244,63 @@ template <typename T, int R> struct PM : PMBase {
     }
 
     // The fused gather/kick/drift + deposit of variant V (FP32, FD4).
+    // TMA staging of the 3D tile's particle arrays (FP32, 32x8x8 tiles):
+    // tensor maps over d[k], p[k] built once at creation.
+    TileMaps tmaps{};
+    bool tma_ok = false;
+    size_t tma_smem = 0;
+
+    int tma_setup() {
+        if constexpr (sizeof(T) == 4 && R == 3) {
+            typedef LagTile<3, 0> L;
+            const char *off = getenv("CONAN_NO_TMA");
+            if ((off && *off && *off != '0') || lag_v != 0) return CONAN_OK;
+            typedef CUresult (*Encode)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                       const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                       CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                       CUtensorMapFloatOOBfill);
+            void *fn = nullptr;
+            cudaDriverEntryPointQueryResult q{};
+            if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+                !fn) {
+                cudaGetLastError();
+                return CONAN_OK;  // no encoder: the kernel reads global memory directly
+            }
+            const cuuint64_t n = (cuuint64_t)mm.n;
+            const cuuint64_t dims[3] = {n, n, n * (cuuint64_t)mm.batch};
+            const cuuint64_t strides[2] = {n * 4, n * n * 4};
+            const cuuint32_t box[3] = {L::LX, L::LY, L::LZ}, estr[3] = {1, 1, 1};
+            float *arr[6] = {P.d[0], P.d[1], P.d[2], P.p[0], P.p[1], P.p[2]};
+            for (int a = 0; a < 6; ++a)
+                if (((Encode)fn)(&tmaps.a[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, arr[a], dims, strides, box, estr,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                    return CONAN_OK;
+            tma_smem = std::max(lag_smem, (size_t)(6 * L::LX * L::LY * L::LZ * 4 + 128));
+            auto kern = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem) != cudaSuccess) {
+                cudaGetLastError();
+                return CONAN_OK;
+            }
+            tma_ok = true;
+        }
+        return CONAN_OK;
+    }
+
     template <int V> int launch_gkd_lag(const GKD &c, const char *name) {
         if constexpr (sizeof(T) == 4) {
             typedef LagTile<R, V> L;
             size_t tiles = (size_t)(mm.n / L::LX) * (R >= 2 ? mm.n / L::LY : 1) * (R == 3 ? mm.n / L::LZ : 1) *
                            (size_t)mm.batch;
+            if constexpr (R == 3 && V == 0) {
+                if (tma_ok) {
+                    auto tk = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
+                    CONAN_TIMED(prof, name, st,
+                                (tk<<<(unsigned)tiles, L::THREADS, tma_smem, st>>>(P, mf, grad, c, lwin, lacc,
+                                                                                   tmaps, err)));
+                    return CONAN_OK;
+                }
+            }
             auto kern = k_gkd_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
             CONAN_TIMED(prof, name, st,
                         (kern<<<(unsigned)tiles, L::THREADS, lag_smem, st>>>(P, mf, grad, c, lwin, lacc)));

@@ -882,10 +882,14 @@ template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1
 // particles are first advanced as in k_gkd (gather of the packed gradient,
 // kick, drift; positions and momenta written back) and the new positions are
 // deposited, so the deposit costs no second pass over the particles.
-template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED>
+// stage: the tile's d[0..2], p[0..2] already copied to shared memory (six
+// LX*LY*LZ arrays in tile order, see k_gkd_lag_tma), or nullptr to read
+// them from global memory.
+template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED, bool STAGED = false>
 __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
                                          unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
-                                         const GKD &gc) {
+                                         const GKD &gc, const float *stage = nullptr) {
+    constexpr int NT = LX * LY * LZ;
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
     constexpr int NW = THREADS / 32;
@@ -922,8 +926,13 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             float p[3];
 #pragma unroll
             for (int k = 0; k < R; ++k) {  // read once: evict-first, L1 stays for the gradients
-                d[k] = __ldcs(P.d[k] + i);
-                p[k] = __ldcs(P.p[k] + i);
+                if constexpr (STAGED) {
+                    d[k] = stage[k * NT + t];
+                    p[k] = stage[(3 + k) * NT + t];
+                } else {
+                    d[k] = __ldcs(P.d[k] + i);
+                    p[k] = __ldcs(P.p[k] + i);
+                }
             }
             if (gc.kick) {
                 float F[3];
@@ -962,6 +971,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             wred[3 + k][wid] = b;
         }
     }
+    if constexpr (STAGED) __syncthreads();  // staged particles are read before the window reuses the memory
     uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
     for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
@@ -1078,6 +1088,66 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     k_gkd_lag(Parts<float> P, Mesh m, const G4<float> *__restrict__ G, GKD gc, LagWin win,
               unsigned long long *__restrict__ acc) {
     lag_tile<R, LX, LY, LZ, THREADS, true>(P, m, win, acc, G, gc);
+}
+
+// ------------------------------------------- TMA staging of a 3D tile --
+//
+// The six particle arrays of a 3D lattice tile (d[0..2], p[0..2], LX x LY x
+// LZ floats each) are one box each of a tensor map over the (N, N, N*batch)
+// array; thread 0 issues the six bulk tensor copies into shared memory and
+// every thread waits on one mbarrier (bounded: after TMA_WAIT_LIMIT polls it
+// sets bit 8 of the error word and goes on), then the tile runs from shared
+// memory. No multicast: every copy reads this GPU's own memory into this CTA.
+struct TileMaps {
+    CUtensorMap a[6];  // d0, d1, d2, p0, p1, p2
+};
+
+constexpr unsigned TMA_WAIT_LIMIT = 1u << 20;  // polls of try_wait (about a second at most)
+
+__device__ inline uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+template <int R, int LX, int LY, int LZ, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+    k_gkd_lag_tma(Parts<float> P, Mesh m, const G4<float> *__restrict__ G, GKD gc, LagWin win,
+                  unsigned long long *__restrict__ acc, const __grid_constant__ TileMaps maps, int *err) {
+    static_assert(R == 3, "the staged tile is three-dimensional");
+    constexpr int NT = LX * LY * LZ;
+    extern __shared__ __align__(16) uint32_t lag_sh[];
+    __shared__ __align__(8) unsigned long long bar;
+    // bulk tensor copies land on 128-byte boundaries (the launch adds 128 bytes)
+    float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(lag_sh) + 127) & ~(uintptr_t)127);
+    const int s = P.mshift;
+    const int ntx = (1 << s) / LX, nty = (1 << s) / LY, ntz = (1 << s) / LZ;
+    const unsigned tiles = (unsigned)(ntx * nty * ntz);
+    const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
+    const int x0 = (int)(tile % ntx) * LX, y0 = (int)((tile / ntx) % nty) * LY;
+    const int z0 = (int)(tile / (ntx * nty)) * LZ + (int)(member << s);
+    const uint32_t b = smem_addr(&bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(6u * NT * 4u)
+                     : "memory");
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(stage + a * NT)),
+                "l"(reinterpret_cast<uint64_t>(&maps.a[a])), "r"(x0), "r"(y0), "r"(z0), "r"(b)
+                : "memory");
+    }
+    uint32_t done = 0;
+    for (unsigned it = 0; it < TMA_WAIT_LIMIT && !done; ++it)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b)
+            : "memory");
+    if (!done && threadIdx.x == 0) atomicOr(err, 8);
+    lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage);
 }
 
 // Density contrast from the integer accumulator (units of 2^-23 particle
