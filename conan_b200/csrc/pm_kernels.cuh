@@ -882,13 +882,16 @@ template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1
 // particles are first advanced as in k_gkd (gather of the packed gradient,
 // kick, drift; positions and momenta written back) and the new positions are
 // deposited, so the deposit costs no second pass over the particles.
-// stage: the tile's d[0..2], p[0..2] already copied to shared memory (six
-// LX*LY*LZ arrays in tile order, see k_gkd_lag_tma), or nullptr to read
-// them from global memory.
+// STAGED: the tile's d[0..2], p[0..2] arrive in shared memory (six
+// LX*LY*LZ arrays in tile order, see k_gkd_lag_tma), particle group j
+// signalled by bars[j]; otherwise they are read from global memory.
+__device__ inline void tma_wait(unsigned long long *bar, int *err);
+
 template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED, bool STAGED = false>
 __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
                                          unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
-                                         const GKD &gc, const float *stage = nullptr) {
+                                         const GKD &gc, const float *stage = nullptr,
+                                         unsigned long long *bars = nullptr, int *err = nullptr) {
     constexpr int NT = LX * LY * LZ;
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
@@ -927,6 +930,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
 #pragma unroll
             for (int k = 0; k < R; ++k) {  // read once: evict-first, L1 stays for the gradients
                 if constexpr (STAGED) {
+                    if (k == 0) tma_wait(bars + j, err);  // group j: this thread's particle j
                     d[k] = stage[k * NT + t];
                     p[k] = stage[(3 + k) * NT + t];
                 } else {
@@ -1093,27 +1097,43 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 // ------------------------------------------- TMA staging of a 3D tile --
 //
 // The six particle arrays of a 3D lattice tile (d[0..2], p[0..2], LX x LY x
-// LZ floats each) are one box each of a tensor map over the (N, N, N*batch)
-// array; thread 0 issues the six bulk tensor copies into shared memory and
-// every thread waits on one mbarrier (bounded: after TMA_WAIT_LIMIT polls it
-// sets bit 8 of the error word and goes on), then the tile runs from shared
-// memory. No multicast: every copy reads this GPU's own memory into this CTA.
+// LZ floats each) come from tensor maps over the (N, N, N*batch) arrays, in
+// NPT groups of LZ/NPT z-planes: group j holds every thread's particle j.
+// Thread 0 issues the bulk tensor copies of all groups at once, each group
+// completing its own mbarrier, and every thread waits for group j just
+// before it needs particle j, so the first particles are computed while the
+// rest arrive. Waits are bounded: after TMA_WAIT_LIMIT polls a wait sets bit
+// 8 of the error word and goes on. No multicast: every copy reads this GPU's
+// own memory into this CTA.
 struct TileMaps {
-    CUtensorMap a[6];  // d0, d1, d2, p0, p1, p2
+    CUtensorMap a[6];  // d0, d1, d2, p0, p1, p2; box LX x LY x (LZ / NPT)
 };
 
 constexpr unsigned TMA_WAIT_LIMIT = 1u << 20;  // polls of try_wait (about a second at most)
 
 __device__ inline uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
+__device__ inline void tma_wait(unsigned long long *bar, int *err) {
+    const uint32_t b = smem_addr(bar);
+    uint32_t done = 0;
+    for (unsigned it = 0; it < TMA_WAIT_LIMIT && !done; ++it)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b)
+            : "memory");
+    if (!done) atomicOr(err, 8);
+}
+
 template <int R, int LX, int LY, int LZ, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     k_gkd_lag_tma(Parts<float> P, Mesh m, const G4<float> *__restrict__ G, GKD gc, LagWin win,
                   unsigned long long *__restrict__ acc, const __grid_constant__ TileMaps maps, int *err) {
     static_assert(R == 3, "the staged tile is three-dimensional");
-    constexpr int NT = LX * LY * LZ;
+    constexpr int NT = LX * LY * LZ, NPT = NT / THREADS, GZ = LZ / NPT;
+    static_assert(GZ * NPT == LZ && GZ * LX * LY == THREADS, "a group of z-planes holds one particle per thread");
     extern __shared__ __align__(16) uint32_t lag_sh[];
-    __shared__ __align__(8) unsigned long long bar;
+    __shared__ __align__(8) unsigned long long bars[NPT];
     // bulk tensor copies land on 128-byte boundaries (the launch adds 128 bytes)
     float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(lag_sh) + 127) & ~(uintptr_t)127);
     const int s = P.mshift;
@@ -1122,32 +1142,28 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
     const int x0 = (int)(tile % ntx) * LX, y0 = (int)((tile / ntx) % nty) * LY;
     const int z0 = (int)(tile / (ntx * nty)) * LZ + (int)(member << s);
-    const uint32_t b = smem_addr(&bar);
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b));
+#pragma unroll
+        for (int j = 0; j < NPT; ++j) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + j)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(6u * NT * 4u)
-                     : "memory");
 #pragma unroll
-        for (int a = 0; a < 6; ++a)
-            asm volatile(
-                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(stage + a * NT)),
-                "l"(reinterpret_cast<uint64_t>(&maps.a[a])), "r"(x0), "r"(y0), "r"(z0), "r"(b)
-                : "memory");
+        for (int j = 0; j < NPT; ++j) {
+            const uint32_t b = smem_addr(bars + j);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(6u * THREADS * 4u)
+                         : "memory");
+#pragma unroll
+            for (int a = 0; a < 6; ++a)
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                    " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(stage + a * NT + j * THREADS)),
+                    "l"(reinterpret_cast<uint64_t>(&maps.a[a])), "r"(x0), "r"(y0), "r"(z0 + j * GZ), "r"(b)
+                    : "memory");
+        }
     }
-    uint32_t done = 0;
-    for (unsigned it = 0; it < TMA_WAIT_LIMIT && !done; ++it)
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(b)
-            : "memory");
-    if (!done && threadIdx.x == 0) atomicOr(err, 8);
-    lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage);
+    lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage, bars, err);
 }
 
 // Density contrast from the integer accumulator (units of 2^-23 particle
