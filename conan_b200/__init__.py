@@ -11,10 +11,12 @@ _lib.lib()  # fail at import time if the native library is missing
 
 from .pm import (  # noqa: E402
     Cosmology,
+    FoF,
     Gravity,
     LeapFrog,
     cic,
     compute_displacement,
+    fof,
     compute_potential,
     generate_random_field,
     ic_params,
@@ -23,6 +25,6 @@ from .pm import (  # noqa: E402
 from .conanfile import ConanFile  # noqa: E402
 
 __all__ = [
-    "ConanError", "ConanFile", "Cosmology", "Gravity", "LeapFrog", "cic", "compute_displacement",
-    "compute_potential", "generate_random_field", "ic_params", "white_noise",
+    "ConanError", "ConanFile", "Cosmology", "FoF", "Gravity", "LeapFrog", "cic", "compute_displacement",
+    "compute_potential", "fof", "generate_random_field", "ic_params", "white_noise",
 ]

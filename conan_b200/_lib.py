@@ -38,6 +38,11 @@ class CicParams(C.Structure):
                 ("sub_sample", C.c_int), ("device", C.c_int)]
 
 
+class FofParams(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n_particles", C.c_ulonglong), ("size", C.c_double),
+                ("linking_length", C.c_double), ("device", C.c_int)]
+
+
 class DiffParams(C.Structure):
     _fields_ = [("ic", ICParams), ("pm", PMParams), ("a0", C.c_double), ("da", C.c_double),
                 ("n", C.c_uint), ("checkpoint_every", C.c_uint)]
@@ -65,6 +70,12 @@ SIGNATURES = {
     "conan_ic_potential": (C.c_int, [C.POINTER(ICParams), _dp]),
     "conan_ic_displacement": (C.c_int, [C.POINTER(ICParams), _dp, _dp]),
     "conan_cic": (C.c_int, [C.POINTER(CicParams), _dp, _dp]),
+    "conan_fof": (C.c_int, [C.POINTER(FofParams), _dp, C.c_void_p, C.POINTER(C.c_ulonglong)]),
+    "conan_fof_create": (C.c_void_p, [C.POINTER(FofParams)]),
+    "conan_fof_destroy": (None, [C.c_void_p]),
+    "conan_fof_run": (C.c_int, [C.c_void_p, _dp, C.c_void_p, C.POINTER(C.c_ulonglong)]),
+    "conan_fof_run_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_ulonglong),
+                                       C.c_void_p]),
     "conan_pm_create": (C.c_void_p, [C.POINTER(PMParams)]),
     "conan_pm_destroy": (None, [C.c_void_p]),
     "conan_pm_init": (C.c_int, [C.c_void_p, _dp, C.c_double, C.c_double]),

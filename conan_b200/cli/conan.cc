@@ -1,5 +1,5 @@
-// conan -- host CLI with the reference's `ic`, `run` and `cic` commands on the
-// GPU.
+// conan -- host CLI with the reference's `ic`, `run`, `cic` and `fof` commands
+// on the GPU.
 //
 // Drop-in for the reference binary's sub-commands (src/base/main.cc:95-119):
 // the same option tables (src/ic/main.cc:15-65, src/run/main.cc:20-61,
@@ -9,13 +9,16 @@
 // displacement]; `run` reads its potential record and writes
 // <id>.pos.<k>.conan every 10 steps (or IFRIT .bin / ASCII .txt),
 // src/run/nbody.hh:135-218; `cic` reads <id>.pos.<m>.conan and writes
-// <id>.rho.<m>.conan (src/cic/main.cc:43-79). The numerics run in
-// libconan_pm.so.
+// <id>.rho.<m>.conan (src/cic/main.cc:43-79); `fof` reads a snapshot and
+// writes the text file <id>.fof.<t>.txt (src/fof/fof.cc:282-333). The
+// numerics run in libconan_pm.so.
 //
 // Options that only this build has (precision, noise source, gradient,
 // device, periodic gather) are marked local: they are parsed like the others
 // but never written into file headers, so files keep the reference's keys.
+#include <algorithm>
 #include <cerrno>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -621,11 +624,169 @@ void cmd_cic(int argc, char **argv) {
     save_record(fo, "density", "float64", rho.data(), rho.size() * sizeof(double));
 }
 
+// --------------------------------------------------------------- fof ----
+
+// timed_filename (src/base/date.cc:34-49): <id>.<stage>.<round(b * 10^4), 5
+// digits>.<ext>, or <id>.<stage>.init.<ext> for b < 0; b is a float.
+std::string timed_filename(const std::string &id, const std::string &stage, float b, const std::string &ext) {
+    std::ostringstream s;
+    if (b < 0.0f)
+        s << id << "." << stage << ".init" << ext;
+    else
+        s << id << "." << stage << "." << std::setfill('0') << std::setw(5) << static_cast<int>(std::round(b * 10000))
+          << ext;
+    return s.str();
+}
+
+// modulus(double, double), src/base/misc.hh:144-148.
+double ref_modulus(double a, double b) {
+    if (a < 0) return a - static_cast<int>(a / b - 1) * b;
+    return a - static_cast<int>(a / b) * b;
+}
+
+// random_colour (src/fof/fof.cc:156-161): srand(t); rand() % 1022. glibc's
+// rand() is random() on a 128-byte state; random_r on a private state of the
+// same size gives the same numbers, so groups are coloured in parallel.
+int group_colour(unsigned seed) {
+    char state[128];
+    struct random_data rd;
+    std::memset(&rd, 0, sizeof rd);
+    initstate_r(seed, state, sizeof state, &rd);
+    int32_t r = 0;
+    random_r(&rd, &r);
+    return r % 1022;
+}
+
+// The text that fof_run writes after the header and history
+// (src/fof/fof.cc:233-279): groups of at least 10 particles as "x y z  mass
+// t" with the first (lowest-index) member's position wrapped by modulus, an
+// empty line pair, then every group's members in index order as "x y z
+// colour" with raw positions. Doubles print as std::ostream does (%g, 6
+// digits). Formatting runs on all host threads in chunks written in order.
+void write_fof(std::ostream &fo, int R, const std::vector<double> &X, const std::vector<unsigned long long> &tags,
+               uint64_t ng, double L) {
+    const size_t n = tags.size();
+    std::vector<uint64_t> start(ng + 1, 0), first(ng, 0), order(n);
+    for (size_t i = 0; i < n; ++i) {
+        const uint64_t t = tags[i];
+        if (t == 0 || t > ng) throw Fail("fof: group tag out of range");
+        if (start[t] == 0) first[t - 1] = i;
+        ++start[t];
+    }
+    for (uint64_t t = 0; t < ng; ++t) start[t + 1] += start[t];  // start[t] = first slot of group t (0-based)
+    {
+        std::vector<uint64_t> fill(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < n; ++i) order[fill[tags[i] - 1]++] = i;
+    }
+    unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<int> colour(ng);
+    {
+        std::vector<std::thread> th;
+        for (unsigned w = 0; w < nt; ++w)
+            th.emplace_back([&, w] {
+                for (uint64_t t = w; t < ng; t += nt) colour[t] = group_colour((unsigned)t);
+            });
+        for (auto &t : th) t.join();
+    }
+    char buf[160];
+    auto vec = [&](char *p, const double *x) {
+        int k = 0;
+        for (int a = 0; a < R; ++a) k += std::snprintf(p + k, sizeof buf - k, "%g ", x[a]);
+        return k;
+    };
+    std::string head;
+    for (uint64_t t = 0; t < ng; ++t) {
+        const uint64_t m = start[t + 1] - start[t];
+        if (m < 10) continue;
+        double x[3];
+        for (int a = 0; a < R; ++a) x[a] = ref_modulus(X[first[t] * R + a], L);
+        int k = vec(buf, x);
+        k += std::snprintf(buf + k, sizeof buf - k, " %llu %llu\n", (unsigned long long)m, (unsigned long long)t);
+        head.append(buf, k);
+    }
+    head += "\n\n";
+    fo << head;
+    const size_t chunk = 1 << 20;
+    for (size_t c0 = 0; c0 < n; c0 += chunk * nt) {
+        std::vector<std::string> out(nt);
+        std::vector<std::thread> th;
+        for (unsigned w = 0; w < nt; ++w)
+            th.emplace_back([&, w] {
+                const size_t b = c0 + w * chunk, e = std::min(n, b + chunk);
+                char lb[160];
+                for (size_t s = b; s < e; ++s) {
+                    const size_t i = order[s];
+                    int k = 0;
+                    for (int a = 0; a < R; ++a) k += std::snprintf(lb + k, sizeof lb - k, "%g ", X[i * R + a]);
+                    k += std::snprintf(lb + k, sizeof lb - k, " %d\n", colour[tags[i] - 1]);
+                    out[w].append(lb, k);
+                }
+            });
+        for (auto &t : th) t.join();
+        for (auto &o : out) fo << o;
+    }
+}
+
+void cmd_fof(int argc, char **argv) {
+    Argv C;
+    C.opts = {
+        {0, "h", "help", "false", "print help on the use of this program."},
+        {Option::VALUED | Option::CHECK, "i", "id", date_string(), "identifier for filenames."},
+        {Option::VALUED | Option::CHECK, "t", "time", "1.0", "time of snapshot."},
+        {Option::VALUED | Option::CHECK, "l", "linking-length", "0.1", "linking length in units of Mpc h^-1."},
+        {Option::VALUED | Option::CHECK, "f", "filename", "", "if given, supersedes internal naming system."},
+        {0, "", "ascii", "true", "give output in ASCII."},
+        {Option::VALUED | Option::CHECK | Option::LOCAL, "", "device", "0", "CUDA device."},
+    };
+    C.parse(argc, argv);
+    if (C.flag("help")) {
+        std::cout << "Cosmic workset Conan (B200 build).\n\n";
+        C.print(std::cout);
+        exit(0);
+    }
+    const double t = C.get<double>("time");
+    const std::string fi_fn = C["filename"].empty() ? timed_filename(C["id"], "pos", (float)t, ".conan") : C["filename"];
+    std::ifstream fi(fi_fn, std::ios::binary);
+    if (!fi) throw Fail("Could not read from file " + fi_fn);
+    Header H;
+    H.from_file(fi);
+    H << C;
+    History I;
+    I.from_file(fi);
+    I.update(C.command_line);
+    const int R = H.count("dim") == 1 ? H.get<int>("dim") : 3;
+    const double L = H.get<double>("L"), ll = H.get<double>("linking-length");
+
+    std::ofstream fo(timed_filename(C["id"], "fof", (float)t, ".txt"));
+    if (!fo) throw Fail("could not write the fof file");
+    fo << "# header\n";
+    for (auto &kv : H) fo << "# " << kv.first << "=" << first_line(kv.second) << "\n";
+    fo << "\n# history\n";
+    for (auto &kv : I) fo << "# " << kv.first << ":" << first_line(kv.second) << "\n";
+    fo << "\n";
+    if (R != 2 && R != 3) return;  // fof_run exists for 2 and 3 dimensions only (src/fof/fof.cc:321-327)
+
+    std::vector<double> X = load_record(fi, "pos");
+    fi.close();
+    const size_t n = X.size() / R;
+    std::vector<unsigned long long> tags(n);
+    unsigned long long ng = 0;
+    conan_fof_params p{};
+    p.dim = R;
+    p.n_particles = n;
+    p.size = L;
+    p.linking_length = ll;
+    p.device = C.get<int>("device");
+    check(conan_fof(&p, X.data(), tags.data(), &ng));
+    std::cerr << "[found " << ng << " groups]\n";
+    write_fof(fo, R, X, tags, ng, L);
+}
+
 void usage(const std::string &cmd) {
     std::cout << "Conan - cosmological tool chain - NBody code (B200 build).\n\n"
                  "This is a very basic N-body code, using Particle-Mesh method.\n\n"
                  "usage: "
-              << cmd << " [command] [args]\nwhere [command] is one of: ic, run, cic\nto get help on a command: " << cmd
+              << cmd << " [command] [args]\nwhere [command] is one of: ic, run, cic, fof\nto get help on a command: " << cmd
               << " [command] --help\n";
 }
 
@@ -636,7 +797,7 @@ int main(int argc, char **argv) {
         usage(argv[0]);
         return 0;
     }
-    std::map<std::string, std::function<void(int, char **)>> commands = {{"ic", cmd_ic}, {"run", cmd_run}, {"cic", cmd_cic}};
+    std::map<std::string, std::function<void(int, char **)>> commands = {{"ic", cmd_ic}, {"run", cmd_run}, {"cic", cmd_cic}, {"fof", cmd_fof}};
     std::string command(argv[1]);
     try {
         auto it = commands.find(command);

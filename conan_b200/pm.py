@@ -112,6 +112,63 @@ def cic(X: np.ndarray, dim: int, n_mass: int, L_box: float, f: int = 2, sub_samp
     return out
 
 
+def _fof_params(dim, n, L_box, linking_length, device):
+    p = L.FofParams()
+    p.dim, p.n_particles, p.size, p.linking_length, p.device = dim, n, float(L_box), float(linking_length), device
+    return p
+
+
+def fof(X: np.ndarray, dim: int, L_box: float, linking_length: float, device: int = 0):
+    """The `fof` tool's groups, fof_run<R> (src/fof/fof.cc:164-231): returns
+    (tags, n_groups) for the positions X (n x dim, not wrapped); tags[i] is
+    particle i's group, numbered from 1 in the order of the groups' lowest
+    particle index, as the reference's tags."""
+    x = np.ascontiguousarray(X, dtype=np.float64)
+    if x.size % dim:
+        raise ValueError(f"positions of shape {x.shape} are not n x {dim}")
+    n = x.size // dim
+    tags = np.empty(n, dtype=np.uint64)
+    ng = C.c_ulonglong(0)
+    L.check(L.lib().conan_fof(C.byref(_fof_params(dim, n, L_box, linking_length, device)), L.ptr(x),
+                              tags.ctypes.data_as(C.c_void_p), C.byref(ng)))
+    return tags, int(ng.value)
+
+
+class FoF:
+    """Friends-of-friends with the device buffers kept between calls
+    (conan_fof_create / conan_fof_run / conan_fof_run_device)."""
+
+    def __init__(self, dim: int, n: int, L_box: float, linking_length: float, device: int = 0):
+        self.dim, self.n = dim, n
+        self.h = L.lib().conan_fof_create(C.byref(_fof_params(dim, n, L_box, linking_length, device)))
+        if not self.h:
+            raise L.ConanError(L.ERR_ALLOC, L.last_error())
+
+    def __call__(self, X: np.ndarray):
+        x = np.ascontiguousarray(X, dtype=np.float64)
+        if x.size != self.n * self.dim:
+            raise ValueError(f"expected {self.n} x {self.dim} positions, got {x.shape}")
+        tags = np.empty(self.n, dtype=np.uint64)
+        ng = C.c_ulonglong(0)
+        L.check(L.lib().conan_fof_run(self.h, L.ptr(x), tags.ctypes.data_as(C.c_void_p), C.byref(ng)))
+        return tags, int(ng.value)
+
+    def run_device(self, x_ptr: int, tags_ptr: int, stream: int = 0) -> int:
+        """Device pointers (n x dim doubles in, n uint64 tags out); returns the group count."""
+        ng = C.c_ulonglong(0)
+        L.check(L.lib().conan_fof_run_device(self.h, C.c_void_p(x_ptr), C.c_void_p(tags_ptr), C.byref(ng),
+                                             C.c_void_p(stream)))
+        return int(ng.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            L.lib().conan_fof_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 class Cosmology:
     """src/run/cosmology.hh:6-28."""
 

@@ -116,6 +116,40 @@ typedef struct {
  * accumulation (2^-40 units), so the result does not depend on the order. */
 int conan_cic(const conan_cic_params *p, const double *X, double *rho_out);
 
+/* ----------------------------------------------------------------- fof -- */
+
+/* Options of the `fof` tool, src/fof/fof.cc:282-333, with the snapshot's box. */
+typedef struct {
+    int dim;                        /* 2 or 3 (fof_run<2>, fof_run<3>) */
+    unsigned long long n_particles; /* particles in the snapshot (< 2^32 - 1) */
+    double size;                    /* box size L */
+    double linking_length;          /* --linking-length, same units as L */
+    int device;                     /* CUDA device ordinal */
+} conan_fof_params;
+
+/* fof_run<R>, src/fof/fof.cc:164-231: friends-of-friends groups of the
+ * positions X (n_particles x dim doubles, AoS, the snapshot's `pos` record,
+ * not wrapped). Two particles are friends when the squared length of their
+ * coordinate difference, wrapped once per axis into [-L/2, L/2], is at most
+ * linking_length^2 (Proximity, src/fof/fof.cc:85-99); groups are the
+ * connected sets of friends. tags[i] receives particle i's group number:
+ * groups are numbered from 1 in the order of their lowest particle index, as
+ * the reference's `tags` array. *n_groups receives the number of groups. */
+int conan_fof(const conan_fof_params *p, const double *X, unsigned long long *tags,
+              unsigned long long *n_groups);
+
+/* The same with the device buffers kept between calls (one problem size). */
+typedef struct conan_fof_engine conan_fof_engine;
+conan_fof_engine *conan_fof_create(const conan_fof_params *p);
+void conan_fof_destroy(conan_fof_engine *h);
+/* Host positions in, host tags out. */
+int conan_fof_run(conan_fof_engine *h, const double *X, unsigned long long *tags, unsigned long long *n_groups);
+/* Device positions in, device tags out, enqueued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream); returns after the group count
+ * is known. */
+int conan_fof_run_device(conan_fof_engine *h, const double *X, unsigned long long *tags,
+                         unsigned long long *n_groups, void *stream);
+
 /* ------------------------------------------------------------------ pm -- */
 
 /* Parameters of the `run` tool, src/run/main.cc:20-61,82-103, as the

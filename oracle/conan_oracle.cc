@@ -737,4 +737,74 @@ void oracle_diff_forward(int R, int mbits, int f, double L, double ns, int smoot
     for (size_t c = 0; c < nc; ++c) delta_out[c] -= 1.0;
 }
 
+/* Friends-of-friends tags, fof_run<R> (src/fof/fof.cc:164-231): for every
+ * particle in index order that has no tag yet, a flood fill with a stack
+ * (flood_fill, src/fof/fof.cc:17-40) paints the particles reachable through
+ * friends with the next group number. Friends: Proximity (src/fof/fof.cc:
+ * 71-99), the raw difference wrapped once per axis, d.sqr() <= ll * ll. The
+ * reference finds the candidates with a kd-tree (src/fof/kdtree.hh) whose box
+ * test prunes only boxes that cannot hold a friend; here a cell list with
+ * cells no smaller than ll (all pairs when L / ll < 3) gives the same set.
+ * Returns the number of groups. */
+unsigned long long oracle_fof(int R, size_t n, double L, double ll, const double *X, unsigned long long *tags) {
+    long long nc = (long long)(L / (ll * (1.0 + 1e-9)));
+    while (nc > 3 && (double)ipow((size_t)nc, R) > 4.0 * (double)n + 64.0) --nc;
+    if (nc < 3) nc = 1;
+    const size_t cells = ipow((size_t)nc, R);
+    std::vector<size_t> head(cells, (size_t)-1), next(n);
+    std::vector<int> cc(n * R);
+    for (size_t i = n; i-- > 0;) {
+        size_t id = 0;
+        for (int k = R - 1; k >= 0; --k) {
+            double w = X[i * R + k] - std::floor(X[i * R + k] / L) * L;
+            long long c = (long long)(w * ((double)nc / L));
+            c = c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+            cc[i * R + k] = (int)c;
+            id = id * (size_t)nc + (size_t)c;
+        }
+        next[i] = head[id];
+        head[id] = i;
+    }
+    const double half = L / 2, rsqr = ll * ll;
+    auto friends = [&](size_t a, size_t b) {
+        double v = 0;
+        for (int k = 0; k < R; ++k) {
+            double e = X[b * R + k] - X[a * R + k], d;
+            if (e > half) d = e - L;
+            else if (e < -half) d = e + L;
+            else d = e;
+            v += d * d;
+        }
+        return v <= rsqr;
+    };
+    for (size_t i = 0; i < n; ++i) tags[i] = 0;
+    unsigned long long current = 1;
+    std::vector<size_t> stack;
+    const int nb = nc == 1 ? 1 : (R == 2 ? 9 : 27);
+    for (size_t start = 0; start < n; ++start) {
+        if (tags[start] != 0) continue;
+        tags[start] = current;
+        stack.push_back(start);
+        while (!stack.empty()) {
+            size_t a = stack.back();
+            stack.pop_back();
+            for (int q = 0; q < nb; ++q) {
+                size_t id = 0;
+                for (int k = R - 1; k >= 0; --k) {
+                    long long c = cc[a * R + k] + (nb == 1 ? 0 : (q / (k == 0 ? 1 : k == 1 ? 3 : 9)) % 3 - 1);
+                    c = c < 0 ? c + nc : (c >= nc ? c - nc : c);
+                    id = id * (size_t)nc + (size_t)c;
+                }
+                for (size_t b = head[id]; b != (size_t)-1; b = next[b]) {
+                    if (tags[b] == current || !friends(a, b)) continue;
+                    tags[b] = current;
+                    stack.push_back(b);
+                }
+            }
+        }
+        ++current;
+    }
+    return current - 1;
+}
+
 }  // extern "C"

@@ -164,3 +164,59 @@ def diff_adjoint(dim, mbits, f, L, ns, smooth, scale, sigma, a0, da, n, noise, d
     lib().oracle_diff_adjoint(dim, mbits, f, _d(L), _d(ns), int(smooth), _d(scale), _d(sigma), _d(H0), _d(Om),
                               _d(OL), _d(a0), _d(da), C.c_uint(n), P(noise), P(deltabar), P(dens), P(gb))
     return dens, gb
+
+
+def fof(dim, L, ll, X):
+    """Friends-of-friends tags and group count (fof_run, src/fof/fof.cc:164-231)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    n = X.size // dim
+    tags = np.empty(n, dtype=np.uint64)
+    f = lib().oracle_fof
+    f.restype = C.c_ulonglong
+    ng = f(dim, C.c_size_t(n), _d(L), _d(ll), P(X), P(tags))
+    return tags, int(ng)
+
+
+def _ref_modulus(a, b):
+    """modulus(double, double), src/base/misc.hh:144-148 (truncating casts)."""
+    return a - int(a / b - 1) * b if a < 0 else a - int(a / b) * b
+
+
+def fof_report(X, tags, L) -> str:
+    """The text fof_run writes after the header and history (src/fof/fof.cc:
+    233-279), from the tags: groups of at least 10 particles with the first
+    member's wrapped position, mass and 0-based number; two newlines; every
+    group's members in index order with random_colour(t) = srand(t);
+    rand() % 1022 (libc's own generator). Doubles as std::ostream prints them
+    (%g)."""
+    libc = C.CDLL(None)
+    X = np.asarray(X, dtype=np.float64)
+    tags = np.asarray(tags, dtype=np.int64)
+    dim = X.shape[1]
+    ng = int(tags.max()) if tags.size else 0
+    order = np.argsort(tags, kind="stable")
+    mass = np.bincount(tags - 1, minlength=ng)
+    first = np.full(ng, -1, dtype=np.int64)
+    first[tags[order[np.r_[0, np.cumsum(mass)[:-1]]]] - 1] = order[np.r_[0, np.cumsum(mass)[:-1]]]
+    vec = lambda x: "".join("%g " % v for v in x)  # noqa: E731
+    out = []
+    for t in range(ng):
+        if mass[t] < 10:
+            continue
+        out.append(vec([_ref_modulus(float(v), L) for v in X[first[t]]]) + " %d %d\n" % (mass[t], t))
+    out.append("\n\n")
+    colour = []
+    for t in range(ng):
+        libc.srand(C.c_uint(t))
+        colour.append(libc.rand() % 1022)
+    for i in order:
+        out.append(vec(X[i]) + " %d\n" % colour[tags[i] - 1])
+    return "".join(out)
+
+
+def fof_text_body(text: str) -> str:
+    """The part of a fof output file after its header and history blocks."""
+    lines = text.split("\n")
+    h = lines.index("# history")
+    e = lines.index("", h)
+    return "\n".join(lines[e + 1:])

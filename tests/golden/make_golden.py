@@ -2,12 +2,13 @@
 
 Runs the reference's own `conan` binary (oracle/_ref/conan_ref, compiled from
 the reference sources by oracle/Makefile) through its public CLI (ic, run,
-cic), and the
+cic, fof), and the
 reference's own md_cic / LinearInterpolation<Gradient> templates through
 oracle/_ref/libconan_ref.so, on small seeded cases. Needs the reference tree
 (only in the build container); the fixtures it writes are committed.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # everything
+    python tests/golden/make_golden.py fof      # fof.npz only, from the committed snapshots
 """
 import ctypes
 import os
@@ -89,9 +90,55 @@ def kernel_goldens():
     np.savez_compressed(HERE / "kernels.npz", **out)
 
 
+# (case, snapshot, linking length in units of the lattice spacing L / N) of
+# the `fof` runs; the snapshots are the committed ones in <case>.npz, or for
+# the 3D case made here (FOF_3D) the reference's own ic + run, kept in fof.npz
+FOF_CASES = [("c1s", "2", 0.2), ("c1s", "2", 0.5), ("c1s", "2", 1.0), ("c4s", "1", 0.4), ("f3s", "2", 0.2),
+             ("f3s", "2", 0.5), ("f3s", "2", 1.1)]
+FOF_3D = ("f3s", "-d 3 -b 4 -L 20 --scale-free -n -1 --potential --seed 5", "-f 1 -a0 0.02 -da 0.049 -n 20")
+
+
+def fof_goldens():
+    """The reference's `fof` text output (src/fof/fof.cc:231-279) on committed snapshots."""
+    exe = str(REF / "conan_ref")
+    out = {}
+    work = tempfile.mkdtemp()
+    try:
+        name3, ica, runa = FOF_3D
+        snaps3, _ = run_cli(name3, ica, runa, work)
+        for k in ("pos2", "mom2", "hdr2"):
+            out[f"{name3}_{k}"] = snaps3[k]
+        for name, snap, llf in FOF_CASES:
+            z = {f"{a}{snap}": out[f"{name}_{a}{snap}"] for a in ("pos", "mom", "hdr")} if name == name3 \
+                else np.load(HERE / f"{name}.npz")
+            hdr = dict(x.split("=", 1) for x in z[f"hdr{snap}"])
+            c = ConanFile(header=hdr, history=[(1700000000, "ran nbody")])
+            c.add("pos", z[f"pos{snap}"])
+            c.add("mom", z[f"mom{snap}"])
+            src = Path(work) / f"{name}.snap.conan"
+            c.write(str(src))
+            ll = repr(llf * float(hdr["L"]) / int(hdr["N"]))
+            key = f"{name}_{snap}_ll{llf}"
+            subprocess.run([exe, "fof", "-f", str(src), "-i", key, "-l", ll], cwd=work, check=True,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            txt = (Path(work) / f"{key}.fof.10000.txt").read_text()
+            out[f"{key}_text"] = np.array(txt)
+            out[f"{key}_ll"] = np.array(ll)
+            out[f"{key}_L"] = np.float64(hdr["L"])
+            out[f"{key}_dim"] = np.int64(hdr["dim"])
+            out[f"{key}_snapshot"] = np.array(f"{name}_pos{snap}" if name == name3 else f"{name}.npz:pos{snap}")
+    finally:
+        shutil.rmtree(work)
+    np.savez_compressed(HERE / "fof.npz", cases=np.array([f"{n}_{s}_ll{f}" for n, s, f in FOF_CASES]), **out)
+
+
 def main():
     if not (REF / "conan_ref").exists():
         subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True)
+    if sys.argv[1:] == ["fof"]:
+        fof_goldens()
+        print("fof fixtures written to", HERE)
+        return
     work = tempfile.mkdtemp()
     try:
         for name, (ica, runa) in CASES.items():
@@ -103,6 +150,7 @@ def main():
     finally:
         shutil.rmtree(work)
     kernel_goldens()
+    fof_goldens()
     print("golden fixtures written to", HERE)
 
 

@@ -124,3 +124,41 @@ def test_ifrit_and_ascii_snapshots(gpu, tmp_path):
     off = 4 + 4 + 4 + (4 + 24 + 4)
     x = np.frombuffer(raw[off + 4: off + 4 + 4 * n], dtype=np.float32)
     assert np.allclose(x, g["pos1"][:, 0], rtol=1e-6, atol=1e-5)
+
+
+def _fof_blocks(text):
+    lines = text.split("\n")
+    h = lines.index("# history")
+    e = lines.index("", h)
+    header = dict(l[2:].split("=", 1) for l in lines[1:h - 1])
+    history = lines[h + 1:e]
+    return header, history, "\n".join(lines[e + 1:])
+
+
+@pytest.mark.parametrize("name", [str(c) for c in np.load(GOLD / "fof.npz")["cases"]])
+def test_fof_tool_reproduces_the_reference_files(gpu, tmp_path, name):
+    """`conan fof -f <snapshot> -i <id> -l <ll>` on the reference's snapshots
+    against the text files its own `fof` wrote: the same groups and lines byte
+    for byte, the same header keys (the input path aside), the same history."""
+    from conan_b200.conanfile import ConanFile
+    g = np.load(GOLD / "fof.npz")
+    snap = str(g[f"{name}_snapshot"])
+    if ":" in snap:
+        f, k = snap.split(":")
+        z = np.load(GOLD / f)
+        pos, mom, hdr = z[k], z["mom" + k[3:]], z["hdr" + k[3:]]
+    else:
+        pos, mom, hdr = g[snap], g[snap.replace("_pos", "_mom")], g[snap.replace("_pos", "_hdr")]
+    c = ConanFile(header=_header_dict(hdr), history=[(1700000000, "ran nbody")])
+    c.add("pos", pos)
+    c.add("mom", mom)
+    c.write(str(tmp_path / "snap.conan"))
+    _run(["fof", "-f", str(tmp_path / "snap.conan"), "-i", name, "-l", str(g[f"{name}_ll"])], tmp_path)
+    got = (tmp_path / f"{name}.fof.10000.txt").read_text()
+    gh, ghist, gbody = _fof_blocks(got)
+    rh, rhist, rbody = _fof_blocks(str(g[f"{name}_text"]))
+    assert gbody == rbody
+    gh.pop("filename"), rh.pop("filename")
+    assert gh == rh
+    assert ghist[0] == rhist[0] and len(ghist) == len(rhist) == 2
+    assert ghist[1].split(":", 1)[1].split()[0] == "fof"

@@ -10,7 +10,7 @@ agreement is to rounding.
 import numpy as np
 import pytest
 
-from conftest import load_golden
+from conftest import GOLDEN as GOLDEN_DIR, load_golden
 
 EdS = (68.5, 1.0, 0.0)
 
@@ -126,3 +126,58 @@ def test_oracle_power_spectrum_of_single_mode(oracle):
     # the c[3] modes of the shell, times L^2/N^4
     assert abs(P[3] - 2 * (N * N / 2) ** 2 / c[3] * L ** 2 / N ** 4) < 1e-9
     assert np.all(P[np.arange(len(P)) != 3] < 1e-20)
+
+
+def _fof_case(name):
+    g = load_golden("fof")
+    snap = str(g[f"{name}_snapshot"])
+    if ":" in snap:
+        f, k = snap.split(":")
+        X = np.load(GOLDEN_DIR / f)[k]
+    else:
+        X = g[snap]
+    return (X, int(g[f"{name}_dim"]), float(g[f"{name}_L"]), float(str(g[f"{name}_ll"])),
+            str(g[f"{name}_text"]))
+
+
+@pytest.mark.parametrize("name", [str(c) for c in load_golden("fof")["cases"]])
+def test_oracle_fof_matches_reference_fof_tool(oracle, name):
+    """The `fof` tool of the reference on snapshots of its own runs: the
+    oracle's groups, written in the reference's text format, give the
+    reference's output file byte for byte after the header and history."""
+    X, dim, L, ll, text = _fof_case(name)
+    tags, ng = oracle.fof(dim, L, ll, X)
+    assert ng == int(tags.max())
+    assert oracle.fof_report(X, tags, L) == oracle.fof_text_body(text)
+
+
+def test_oracle_fof_cell_list_equals_all_pairs(oracle):
+    """The oracle's cell list finds the same friends as testing every pair
+    (positions outside the box, both cell-list regimes)."""
+    rng = np.random.default_rng(3)
+    for dim, n, L, ll in [(3, 400, 10.0, 0.9), (3, 300, 10.0, 4.0), (2, 500, 7.0, 0.3), (2, 200, 7.0, 3.0)]:
+        X = rng.uniform(-0.6 * L, 1.6 * L, size=(n, dim))
+        X[n // 2:] = X[:n // 2] + rng.normal(0, ll / 2, size=(n - n // 2, dim))  # close pairs
+        tags, ng = oracle.fof(dim, L, ll, X)
+        # all pairs with the reference's predicate, groups by union-find with min-index roots
+        par = np.arange(n)
+
+        def find(a):
+            while par[a] != a:
+                a = par[a]
+            return a
+        for i in range(n):
+            e = X - X[i]
+            d = np.where(e > L / 2, e - L, np.where(e < -L / 2, e + L, e))
+            v = np.zeros(n)
+            for k in range(dim):
+                v = v + d[:, k] * d[:, k]
+            for j in np.nonzero(v <= ll * ll)[0]:
+                a, b = find(i), find(j)
+                if a != b:
+                    par[max(a, b)] = min(a, b)
+        roots = np.array([find(i) for i in range(n)])
+        _, first = np.unique(roots, return_index=True)
+        number = {roots[f]: k + 1 for k, f in enumerate(sorted(first))}
+        assert ng == len(first)
+        assert np.array_equal(tags, np.array([number[r] for r in roots], dtype=np.uint64))
