@@ -21,7 +21,7 @@
 //            and no fused multiply-add; a linked pair joins two trees of a
 //            lock-free union-find that always hooks the larger root under the
 //            smaller one, so every root is the lowest index of its tree;
-//   compress every particle points at its root;
+//   roots    every particle's root (a read-only walk once the links are in);
 //   number   exclusive scan of the root flags = group number - 1.
 #include <algorithm>
 #include <cmath>
@@ -183,21 +183,28 @@ __global__ void __launch_bounds__(FOF_T) k_fof_link(const double *__restrict__ S
     }
 }
 
-// Every particle points at its root; flag = 1 for roots.
-__global__ void __launch_bounds__(FOF_T) k_fof_compress(uint32_t *par, size_t n, uint32_t *__restrict__ flag) {
+// Every particle's root into a separate array, flag = 1 for roots. The walk
+// only reads the parents: a path-halving store in this pass could overwrite
+// a root another thread has just written with an older ancestor.
+__global__ void __launch_bounds__(FOF_T) k_fof_roots(const uint32_t *__restrict__ par, size_t n,
+                                                     uint32_t *__restrict__ root, uint32_t *__restrict__ flag) {
     const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
     if (i >= n) return;
-    const uint32_t r = fof_find(par, (uint32_t)i);
-    __stcg(par + i, r);
+    uint32_t r = (uint32_t)i, p = par[r];
+    while (p != r) {
+        r = p;
+        p = par[r];
+    }
+    root[i] = r;
     flag[i] = r == (uint32_t)i ? 1u : 0u;
 }
 
-__global__ void __launch_bounds__(FOF_T) k_fof_tags(const uint32_t *__restrict__ par,
+__global__ void __launch_bounds__(FOF_T) k_fof_tags(const uint32_t *__restrict__ root,
                                                     const uint32_t *__restrict__ gnum, size_t n,
                                                     unsigned long long *__restrict__ tags) {
     const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
     if (i >= n) return;
-    tags[i] = (unsigned long long)gnum[par[i]] + 1ull;
+    tags[i] = (unsigned long long)gnum[root[i]] + 1ull;
 }
 
 inline unsigned blocks(size_t n) { return (unsigned)((n + FOF_T - 1) / FOF_T); }
@@ -292,10 +299,11 @@ struct FofEngine {
         scan(count, cells, off, s);
         k_fof_scatter<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, cell, slot, off, order, S, par);
         k_fof_link<RR><<<blocks(n), FOF_T, 0, s>>>(S, order, off, n, g, par, err);
-        // root flags into `slot` (free after the scatter), group numbers into `cell`
-        k_fof_compress<<<blocks(n), FOF_T, 0, s>>>(par, n, slot);
+        // roots into `order` and root flags into `slot` (both free after the
+        // link), group numbers into `cell`
+        k_fof_roots<<<blocks(n), FOF_T, 0, s>>>(par, n, order, slot);
         scan(slot, n, cell, s);
-        k_fof_tags<<<blocks(n), FOF_T, 0, s>>>(par, cell, n, tg);
+        k_fof_tags<<<blocks(n), FOF_T, 0, s>>>(order, cell, n, tg);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
             return set_error(CONAN_ERR_CUDA, "fof kernel launch failed: %s", cudaGetErrorString(e));
