@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-cic", action="store_true")
+    ap.add_argument("--no-fof", action="store_true")
     return ap.parse_args()
 
 
@@ -169,6 +170,95 @@ def max_over_ranks(x, dist, device="cuda"):
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+# ------------------------------------------------------------------- fof --
+def fof_bench(cb, Xh, n, dev, steps, reps=3):
+    """The `fof` tool's groups (b = 0.2 linking length) on the final 512^3
+    snapshot: device positions to device tags (conan_fof_run_device, CUDA
+    events, inputs resident in HBM), and end to end through conan_fof_run with
+    host buffers. Size-independent checks: the same tags on every run, and the
+    numbering of the groups in order of their lowest particle index."""
+    import numpy as np
+    import torch
+    Np = n ** 3
+    ll = 0.2 * L_BOX / n
+    eng = cb.FoF(3, Np, L_BOX, ll, device=dev)
+    xd = torch.from_numpy(Xh).to(f"cuda:{dev}")
+    td = torch.empty(Np, dtype=torch.int64, device=f"cuda:{dev}")
+    s = torch.cuda.current_stream(dev)
+    ng = eng.run_device(xd.data_ptr(), td.data_ptr(), s.cuda_stream)  # warm-up
+    first = td.clone()
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ng = eng.run_device(xd.data_ptr(), td.data_ptr(), s.cuda_stream)
+        e1.record(s)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    cm = torch.cummax(td, 0)[0]
+    numbering_ok = bool(td[0].item() == 1 and torch.equal(td, first) and cm[-1].item() == ng and
+                        bool(((cm[1:] - cm[:-1]) <= 1).all().item()) and bool((td <= cm).all().item()))
+    mass = torch.bincount(td - 1)
+    big = int((mass >= 10).sum().item())
+    largest = int(mass.max().item())
+    del xd, td, first, cm, mass
+    tags_h = np.empty(Np, dtype=np.uint64)
+    eng(Xh)  # warm-up of the host path
+    t0 = time.perf_counter()
+    tags_h, _ = eng(Xh)
+    e2e_s = time.perf_counter() - t0
+    eng.close()
+    return {"workload": f"final {n}^3 FP32 snapshot ({steps} steps from a={A0}, da={DA}), b=0.2: linking length 0.2 L/N",
+            "linking_length": ll, "ms": min(ms), "particles_per_s": Np / (min(ms) * 1e-3),
+            "groups": ng, "groups_ge_10": big, "largest_group": largest, "checks_ok": numbering_ok,
+            "e2e": {"particles_per_s": Np / e2e_s, "seconds": e2e_s, "h2d_bytes": Xh.nbytes,
+                    "d2h_bytes": tags_h.nbytes, "what": "conan_fof_run: host positions in, host tags out"}}
+
+
+def fof_tool_vs_reference(cb, n_sample=64, max_seconds=60.0):
+    """The whole `fof` tool (snapshot file in, text file out) on a 64^3 box
+    with the throughput box's spacing (L = 62.5 Mpc/h) run to a = 1 on the GPU:
+    the reference's binary (oracle/_ref/conan_ref, single-threaded kd-tree)
+    against this build's `conan fof`, same file and options; the two text
+    outputs must agree after the header and history."""
+    import tempfile
+    import numpy as np
+    from conan_b200.conanfile import ConanFile
+    mb = int(math.log2(n_sample))
+    L = L_BOX * n_sample / 512
+    H = {"dim": 3, "mbits": mb, "size": L, "ns": NS, "smooth": 0, "scale-free": 1, "scale": 8.0, "sigma": 0.83,
+         "seed": 5}
+    phi = cb.compute_potential(H, cb.generate_random_field(H, precision="fp64"), precision="fp64")
+    g = cb.Gravity(3, n_sample, 1, L, precision="fp32")
+    g.run(phi, A0, DA, 20)
+    X, P = g.state()
+    g.close()
+    ref = ROOT / "oracle" / "_ref" / "conan_ref"
+    out = {"sample": f"{n_sample}^3 particles, L={L}, 20 steps a=0.05->1, b=0.2"}
+    with tempfile.TemporaryDirectory() as w:
+        c = ConanFile(header={"L": repr(L), "N": str(n_sample), "dim": "3"})
+        c.update_history("bench snapshot")
+        c.add("pos", X)
+        c.add("mom", P)
+        c.write(f"{w}/s.conan")
+        args = ["fof", "-f", f"{w}/s.conan", "-l", repr(0.2 * L / n_sample)]
+        t0 = time.perf_counter()
+        subprocess.run([str(ROOT / "conan_b200" / "bin" / "conan"), *args, "-i", "gpu"], cwd=w, check=True,
+                       capture_output=True)
+        out["gpu_tool_s"] = time.perf_counter() - t0
+        if ref.exists():
+            t0 = time.perf_counter()
+            r = subprocess.run([str(ref), *args, "-i", "ref"], cwd=w, capture_output=True,
+                               timeout=max_seconds * 10)
+            out["reference_tool_s"] = time.perf_counter() - t0
+            if r.returncode == 0:
+                body = [open(f"{w}/{k}.fof.10000.txt").read().split("\n# history\n", 1)[1].split("\n\n", 1)[1]
+                        for k in ("gpu", "ref")]
+                out["outputs_identical"] = body[0] == body[1]
+            out["reference_cores"] = 1
+    return out
 
 
 # ------------------------------------------------------------- reference --
@@ -404,6 +494,13 @@ def run_ours(args):
         cic["what"] = ("conan_cic on the final 512^3 FP32 snapshot, f=1 (512^3 mesh), s=1 and s=2 (1024^3 "
                        "interpolated points); host positions in, host density out")
 
+    # the fof tool on the final snapshot, and the whole tool against the reference's
+    fof = None
+    if rank == 0 and not args.no_fof:
+        fof = fof_bench(cb, Xh, n, dev, args.steps)
+        if not args.no_cpu:
+            fof["tool_64"] = fof_tool_vs_reference(cb)
+
     adjoint = None
     if not args.no_adjoint and rank == 0:
         try:
@@ -466,6 +563,7 @@ def run_ours(args):
             "adjoint": adjoint,
             "ensemble": ensemble,
             "cic": cic,
+            "fof": fof,
             "e2e": {"value": world * Np * args.steps / e2e_s, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": phi.nbytes / args.steps,
                     "d2h_bytes_per_step": (Xh.nbytes + Ph.nbytes) / args.steps,

@@ -8,25 +8,32 @@
 // (the flood fill started from every untagged particle in index order,
 // src/fof/fof.cc:183-231). The result is a partition plus that numbering, so
 // any order of discovery gives the same tags. Here:
-//   bin      every particle's cell on a grid whose cells are no smaller than
-//            the linking length (wrapped coordinates) and its rank in the
-//            cell from an integer counter;
-//   scan     cell offsets;
-//   scatter  particle indices and coordinates (one array per axis) in cell
-//            order;
-//   link     one thread per sorted particle tests the particles after it in
-//            its own cell and all particles of the (3^R - 1) / 2 neighbour
-//            cells that lie ahead of its cell, so every pair within reach is
-//            tested exactly once, in FP64 with the reference's operation order
-//            and no fused multiply-add; a linked pair joins two trees of a
+//   keys     every particle's row -- its cell in the transverse axes (y, or
+//            y and z) on a grid of cells no smaller than the linking length,
+//            wrapped coordinates -- and its wrapped x quantised to 2^16
+//            steps, as one 64-bit key; an integer count per row;
+//   sort     stable radix sort of (key, particle index) (radix.cuh): rows in
+//            order, x ascending inside a row; row offsets from the counts;
+//   gather   coordinates (one array per axis) in sorted order;
+//   link     one thread per sorted particle tests, in its own row, the
+//            particles ahead of it in cyclic x order within the linking
+//            length, and in the forward half of the neighbouring rows
+//            ((3^(R-1) - 1) / 2 rows) those within the linking length in x,
+//            found by binary search; every pair within reach is tested
+//            exactly once, in FP64 with the reference's operation order and
+//            no fused multiply-add. A linked pair joins two trees of a
 //            lock-free union-find that always hooks the larger root under the
 //            smaller one, so every root is the lowest index of its tree;
 //   roots    every particle's root (a read-only walk once the links are in);
 //   number   exclusive scan of the root flags = group number - 1.
+// Against cubic cells, the row-and-window search tests candidates from a
+// volume of 2 ll x (3 ll)^(R-1) around each particle instead of (3 h)^R with
+// cells h >= ll; inside halos that is most of the work.
 #include <algorithm>
 #include <cmath>
 
 #include "pm.cuh"
+#include "radix.cuh"
 #include "scan.cuh"
 
 namespace conan {
@@ -34,30 +41,41 @@ namespace {
 
 constexpr int FOF_T = 256;
 constexpr int FOF_UNITE_LIMIT = 1 << 24;  // retries of one union (each one is another thread's hook)
+constexpr int FOF_XB = 16;                 // bits of the quantised x in the sort key
+constexpr uint32_t FOF_XN = 1u << FOF_XB;
+constexpr uint64_t FOF_XMASK = FOF_XN - 1;
+constexpr uint32_t FOF_NONE = 0xffffffffu;
 
 struct FofGrid {
-    int nc;        // cells per side (1 or >= 3)
-    double L;      // box size
-    double half;   // L / 2
-    double inv_h;  // nc / L
-    double rsqr;   // linking length squared
+    int nr;         // row cells per transverse axis (1 or >= 3)
+    int wq;         // x window in quanta; whole rows when 2 wq + 1 >= 2^16
+    double L;       // box size
+    double half;    // L / 2
+    double inv_h;   // nr / L
+    double xscale;  // 2^16 / L
+    double rsqr;    // linking length squared
 };
 
-// Cell of a position: the coordinate wrapped into [0, L), nc cells per side.
-// Explicitly rounded operations, so that the binning and the link kernel
-// (which recomputes it) agree bit for bit.
+// Wrapped coordinate in [0, L], explicitly rounded.
+__device__ inline double fof_wrap(double x, const FofGrid &g) {
+    return __dsub_rn(x, __dmul_rn(floor(__ddiv_rn(x, g.L)), g.L));
+}
+
+// Row of a position (transverse cells, highest axis most significant) and
+// its key: row << 16 | quantised x.
 template <int R>
-__device__ inline uint32_t fof_cell(const double *x, const FofGrid &g, int *c) {
-    uint32_t id = 0;
+__device__ inline uint64_t fof_key(const double *x, const FofGrid &g, uint32_t *row_out) {
+    uint32_t row = 0;
 #pragma unroll
-    for (int k = R - 1; k >= 0; --k) {
-        const double w = __dsub_rn(x[k], __dmul_rn(floor(__ddiv_rn(x[k], g.L)), g.L));
-        int ck = (int)__dmul_rn(w, g.inv_h);
-        ck = ck < 0 ? 0 : (ck >= g.nc ? g.nc - 1 : ck);
-        c[k] = ck;
-        id = id * (uint32_t)g.nc + (uint32_t)ck;
+    for (int k = R - 1; k >= 1; --k) {
+        int ck = (int)__dmul_rn(fof_wrap(x[k], g), g.inv_h);
+        ck = ck < 0 ? 0 : (ck >= g.nr ? g.nr - 1 : ck);
+        row = row * (uint32_t)g.nr + (uint32_t)ck;
     }
-    return id;
+    long long q = (long long)__dmul_rn(fof_wrap(x[0], g), g.xscale);
+    q = q < 0 ? 0 : (q >= (long long)FOF_XN ? (long long)FOF_XN - 1 : q);
+    *row_out = row;
+    return ((uint64_t)row << FOF_XB) | (uint64_t)q;
 }
 
 // Proximity::operator()(size_t), src/fof/fof.cc:85-99: b = x_j - x_i, one
@@ -91,95 +109,162 @@ __device__ inline uint32_t fof_find(uint32_t *par, uint32_t x) {
 
 // Joins the trees of a and b: the larger root is hooked under the smaller
 // one with a compare-and-swap that only succeeds while it is still a root.
-__device__ inline bool fof_unite(uint32_t *par, uint32_t a, uint32_t b) {
+// Returns the root of the joined tree as this thread last saw it (a cheap
+// starting point for the next union of the same particle), FOF_NONE if it
+// gave up.
+__device__ inline uint32_t fof_unite(uint32_t *par, uint32_t a, uint32_t b) {
     for (int it = 0; it < FOF_UNITE_LIMIT; ++it) {
         a = fof_find(par, a);
         b = fof_find(par, b);
-        if (a == b) return true;
-        if (a < b) {
-            const uint32_t t = a;
-            a = b;
-            b = t;
-        }
-        const uint32_t old = atomicCAS(par + a, a, b);
-        if (old == a) return true;
-        a = old;  // hooked by another thread meanwhile: continue from there
+        if (a == b) return a;
+        const uint32_t hi = a > b ? a : b, lo = a > b ? b : a;
+        const uint32_t old = atomicCAS(par + hi, hi, lo);
+        if (old == hi) return lo;
+        a = old;  // hi was hooked by another thread meanwhile: continue from there
+        b = lo;
     }
-    return false;
+    return FOF_NONE;
 }
 
 template <int R>
-__global__ void __launch_bounds__(FOF_T) k_fof_bin(const double *__restrict__ X, size_t n, FofGrid g,
-                                                   uint32_t *__restrict__ cell, uint32_t *__restrict__ slot,
-                                                   uint32_t *__restrict__ count) {
+__global__ void __launch_bounds__(FOF_T) k_fof_keys(const double *__restrict__ X, size_t n, FofGrid g,
+                                                    uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                    uint32_t *__restrict__ rowcount) {
     const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
     if (i >= n) return;
     double x[3];
-    int c[3];
 #pragma unroll
     for (int k = 0; k < R; ++k) x[k] = X[i * R + k];
-    const uint32_t id = fof_cell<R>(x, g, c);
-    cell[i] = id;
-    slot[i] = atomicAdd(count + id, 1u);
+    uint32_t row;
+    keys[i] = fof_key<R>(x, g, &row);
+    vals[i] = (uint32_t)i;
+    atomicAdd(rowcount + row, 1u);
 }
 
 template <int R>
-__global__ void __launch_bounds__(FOF_T) k_fof_scatter(const double *__restrict__ X, size_t n,
-                                                       const uint32_t *__restrict__ cell,
-                                                       const uint32_t *__restrict__ slot,
-                                                       const uint32_t *__restrict__ off,
-                                                       uint32_t *__restrict__ order, double *__restrict__ S,
-                                                       uint32_t *__restrict__ par) {
-    const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
-    if (i >= n) return;
-    const size_t t = (size_t)off[cell[i]] + slot[i];
-    order[t] = (uint32_t)i;
+__global__ void __launch_bounds__(FOF_T) k_fof_gather(const double *__restrict__ X, size_t n,
+                                                      const uint32_t *__restrict__ order, double *__restrict__ S,
+                                                      uint32_t *__restrict__ par) {
+    const size_t t = (size_t)blockIdx.x * FOF_T + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t i = order[t];
 #pragma unroll
-    for (int k = 0; k < R; ++k) S[(size_t)k * n + t] = X[i * R + k];
-    par[i] = (uint32_t)i;
+    for (int k = 0; k < R; ++k) S[(size_t)k * n + t] = X[(size_t)i * R + k];
+    par[t] = (uint32_t)t;  // every particle its own parent (par is indexed by particle)
 }
 
-// Tests sorted particle t against the particles u in [u0, u1) of one cell.
+struct FofLink {
+    const double *S;
+    const uint64_t *keys;
+    const uint32_t *order;
+    const uint32_t *rowoff;
+    size_t n;
+    FofGrid g;
+    uint32_t *par;
+    int *err;
+};
+
+// Tests sorted particle t (coordinates xi, index i, last known root ri)
+// against sorted particle u.
 template <int R>
-__device__ inline void fof_test_range(const double *xi, uint32_t i, size_t u0, size_t u1, size_t n,
-                                      const double *__restrict__ S, const uint32_t *__restrict__ order,
-                                      const FofGrid &g, uint32_t *par, int *err) {
-    for (size_t u = u0; u < u1; ++u) {
-        double xj[3];
+__device__ inline void fof_test(const FofLink &a, const double *xi, uint32_t i, uint32_t &ri, size_t u) {
+    double xj[3];
 #pragma unroll
-        for (int k = 0; k < R; ++k) xj[k] = __ldg(S + (size_t)k * n + u);
-        if (fof_linked<R>(xi, xj, g) && !fof_unite(par, i, __ldg(order + u))) atomicOr(err, 1);
+    for (int k = 0; k < R; ++k) xj[k] = __ldg(a.S + (size_t)k * a.n + u);
+    if (!fof_linked<R>(xi, xj, a.g)) return;
+    ri = fof_unite(a.par, ri, __ldg(a.order + u));
+    if (ri == FOF_NONE) {
+        atomicOr(a.err, 1);
+        ri = i;
+    }
+}
+
+// Tests the particles of sorted range [u, end) whose quantised x is at most
+// qmax (keys are sorted, so the run stops at the first larger one).
+template <int R>
+__device__ inline void fof_run_to(const FofLink &a, const double *xi, uint32_t i, uint32_t &ri, size_t u, size_t end,
+                                  uint64_t kmax) {
+    for (; u < end && __ldg(a.keys + u) <= kmax; ++u) fof_test<R>(a, xi, i, ri, u);
+}
+
+// First sorted position in [lo, hi) whose key is >= k.
+__device__ inline size_t fof_lower(const uint64_t *keys, size_t lo, size_t hi, uint64_t k) {
+    while (lo < hi) {
+        const size_t mid = lo + ((hi - lo) >> 1);
+        if (__ldg(keys + mid) < k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Tests the particles of row `row` whose quantised x lies in [qa, qb].
+template <int R>
+__device__ inline void fof_row_segment(const FofLink &a, const double *xi, uint32_t i, uint32_t &ri, size_t rs,
+                                       size_t re, uint64_t rk, long long qa, long long qb) {
+    const size_t u = fof_lower(a.keys, rs, re, rk | (uint64_t)qa);
+    fof_run_to<R>(a, xi, i, ri, u, re, rk | (uint64_t)qb);
+}
+
+// The x window [xq - wq, xq + wq] (cyclic) of one neighbour row.
+template <int R>
+__device__ inline void fof_row_window(const FofLink &a, const double *xi, uint32_t i, uint32_t &ri, uint32_t row,
+                                      long long xq, bool whole) {
+    const size_t rs = a.rowoff[row], re = a.rowoff[row + 1];
+    if (rs == re) return;
+    const uint64_t rk = (uint64_t)row << FOF_XB;
+    if (whole) {
+        for (size_t u = rs; u < re; ++u) fof_test<R>(a, xi, i, ri, u);
+        return;
+    }
+    const long long lo = xq - a.g.wq, hi = xq + a.g.wq, N = FOF_XN;
+    if (lo < 0) {
+        fof_row_segment<R>(a, xi, i, ri, rs, re, rk, lo + N, N - 1);
+        fof_row_segment<R>(a, xi, i, ri, rs, re, rk, 0, hi);
+    } else if (hi >= N) {
+        fof_row_segment<R>(a, xi, i, ri, rs, re, rk, lo, N - 1);
+        fof_row_segment<R>(a, xi, i, ri, rs, re, rk, 0, hi - N);
+    } else {
+        fof_row_segment<R>(a, xi, i, ri, rs, re, rk, lo, hi);
     }
 }
 
 template <int R>
-__global__ void __launch_bounds__(FOF_T) k_fof_link(const double *__restrict__ S,
-                                                    const uint32_t *__restrict__ order,
-                                                    const uint32_t *__restrict__ off, size_t n, FofGrid g,
-                                                    uint32_t *par, int *err) {
+__global__ void __launch_bounds__(FOF_T) k_fof_link(FofLink a) {
     const size_t t = (size_t)blockIdx.x * FOF_T + threadIdx.x;
-    if (t >= n) return;
+    if (t >= a.n) return;
     double xi[3];
-    int c[3];
 #pragma unroll
-    for (int k = 0; k < R; ++k) xi[k] = S[(size_t)k * n + t];
-    const uint32_t i = order[t];
-    const uint32_t own = fof_cell<R>(xi, g, c);
-    fof_test_range<R>(xi, i, t + 1, off[own + 1], n, S, order, g, par, err);
-    if (g.nc == 1) return;
-    // the neighbour offsets o in {-1,0,1}^R whose last non-zero component
-    // (highest axis first) is +1: half of the 3^R - 1 neighbours
-    constexpr int NB = (R == 2 ? 9 : 27);
-    for (int q = NB / 2 + 1; q < NB; ++q) {
-        int o[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
-        uint32_t id = 0;
+    for (int k = 0; k < R; ++k) xi[k] = a.S[(size_t)k * a.n + t];
+    const uint32_t i = a.order[t];
+    uint32_t ri = i;
+    const uint64_t key = a.keys[t];
+    const uint32_t row = (uint32_t)(key >> FOF_XB);
+    const long long xq = (long long)(key & FOF_XMASK);
+    const bool whole = 2 * (long long)a.g.wq + 1 >= (long long)FOF_XN;
+    const size_t rs = a.rowoff[row], re = a.rowoff[row + 1];
+    // own row: the particles ahead of t in cyclic x order, up to wq ahead
+    if (whole) {
+        for (size_t u = t + 1; u < re; ++u) fof_test<R>(a, xi, i, ri, u);
+    } else {
+        const uint64_t rk = (uint64_t)row << FOF_XB;
+        const long long hi = xq + a.g.wq;
+        fof_run_to<R>(a, xi, i, ri, t + 1, re, rk | (uint64_t)(hi < (long long)FOF_XN ? hi : (long long)FOF_XN - 1));
+        if (hi >= (long long)FOF_XN) fof_run_to<R>(a, xi, i, ri, rs, t, rk | (uint64_t)(hi - FOF_XN));
+    }
+    if (a.g.nr == 1) return;
+    // the forward half of the neighbouring rows: y + 1 (2D); (y+-1, z+1),
+    // (y, z+1), (y+1, z) (3D)
+    const int nr = a.g.nr;
+    const int cy = (int)(row % (uint32_t)nr), cz = R == 3 ? (int)(row / (uint32_t)nr) : 0;
+    constexpr int NF = R == 2 ? 1 : 4;
+    const int dy[4] = {1, -1, 0, 1}, dz[4] = {0, 1, 1, 1};
 #pragma unroll
-        for (int k = R - 1; k >= 0; --k) {
-            int ck = c[k] + o[k];
-            ck = ck < 0 ? ck + g.nc : (ck >= g.nc ? ck - g.nc : ck);
-            id = id * (uint32_t)g.nc + (uint32_t)ck;
-        }
-        fof_test_range<R>(xi, i, off[id], off[id + 1], n, S, order, g, par, err);
+    for (int f = 0; f < NF; ++f) {
+        int y = cy + dy[f], z = cz + dz[f];
+        y = y < 0 ? y + nr : (y >= nr ? y - nr : y);
+        z = z >= nr ? z - nr : z;
+        const uint32_t nrow = R == 2 ? (uint32_t)y : (uint32_t)z * (uint32_t)nr + (uint32_t)y;
+        fof_row_window<R>(a, xi, i, ri, nrow, xq, whole);
     }
 }
 
@@ -213,30 +298,25 @@ inline unsigned blocks(size_t n) { return (unsigned)((n + FOF_T - 1) / FOF_T); }
 
 // Grid and device buffers of one problem size; reused across runs.
 struct FofEngine {
-    int R = 3, device = 0;
-    size_t n = 0, cells = 0;
+    int R = 3, device = 0, key_bits = 0;
+    size_t n = 0, rows = 0;
     FofGrid g{};
     cudaStream_t st = nullptr;
     double *X = nullptr, *S = nullptr;
-    uint32_t *cell = nullptr, *slot = nullptr, *order = nullptr, *par = nullptr, *count = nullptr,
-             *off = nullptr, *bsum = nullptr;
+    uint64_t *keys[2] = {nullptr, nullptr};
+    uint32_t *vals[2] = {nullptr, nullptr};
+    uint32_t *par = nullptr, *rowcount = nullptr, *rowoff = nullptr, *flag = nullptr, *gnum = nullptr,
+             *bh = nullptr, *boff = nullptr, *bsum = nullptr;
     unsigned long long *tags = nullptr;
     uint32_t *ngroups_h = nullptr;  // pinned
     int *err = nullptr;
 
     ~FofEngine() {
         if (st) cudaStreamSynchronize(st);
-        cudaFree(X);
-        cudaFree(S);
-        cudaFree(cell);
-        cudaFree(slot);
-        cudaFree(order);
-        cudaFree(par);
-        cudaFree(count);
-        cudaFree(off);
-        cudaFree(bsum);
-        cudaFree(tags);
-        cudaFree(err);
+        for (void *q : {(void *)X, (void *)S, (void *)keys[0], (void *)keys[1], (void *)vals[0], (void *)vals[1],
+                        (void *)par, (void *)rowcount, (void *)rowoff, (void *)flag, (void *)gnum, (void *)bh,
+                        (void *)boff, (void *)bsum, (void *)tags, (void *)err})
+            cudaFree(q);
         cudaFreeHost(ngroups_h);
         if (st) cudaStreamDestroy(st);
     }
@@ -245,41 +325,55 @@ struct FofEngine {
         R = p.dim;
         device = p.device;
         n = (size_t)p.n_particles;
-        // cells no smaller than the linking length (with a margin far above
-        // the rounding of the wrap), at most about one per particle
-        double q = p.size / (p.linking_length * (1.0 + 1e-9));
-        long long nc = q >= 2147483647.0 ? 2147483647LL : (long long)q;
+        // transverse cells no smaller than the linking length (with a margin
+        // far above the rounding of the wrap), at most about eight rows per
+        // particle
+        const double q = p.size / (p.linking_length * (1.0 + 1e-9));
+        long long nr = q >= 2147483647.0 ? 2147483647LL : (long long)q;
         long long cap = 1;
         while (true) {
             long long c1 = cap + 1, v = 1;
-            for (int k = 0; k < R; ++k) v *= c1;
-            if (v > (long long)std::max<size_t>(n, 27) || v > (1LL << 30)) break;
+            for (int k = 1; k < R; ++k) v *= c1;
+            if (v > 8 * (long long)std::max<size_t>(n, 27) || v > (1LL << 26)) break;
             cap = c1;
         }
-        nc = std::min(nc, cap);
-        if (nc < 3) nc = 1;
-        g.nc = (int)nc;
+        nr = std::min(nr, cap);
+        if (nr < 3) nr = 1;
+        g.nr = (int)nr;
         g.L = p.size;
         g.half = p.size / 2;
-        g.inv_h = (double)nc / p.size;
+        g.inv_h = (double)nr / p.size;
+        g.xscale = (double)FOF_XN / p.size;
         g.rsqr = p.linking_length * p.linking_length;
-        cells = 1;
-        for (int k = 0; k < R; ++k) cells *= (size_t)nc;
-        const size_t nb = (std::max(cells, n) + SCAN_CHUNK - 1) / SCAN_CHUNK;
+        const double wq = std::ceil(p.linking_length * g.xscale) + 2.0;
+        g.wq = wq >= (double)FOF_XN ? (int)FOF_XN : (int)wq;
+        rows = 1;
+        for (int k = 1; k < R; ++k) rows *= (size_t)nr;
+        int rb = 0;
+        while (((size_t)1 << rb) < rows) ++rb;
+        key_bits = FOF_XB + rb;
+        const size_t tiles = radix_tiles(n), m = 256 * tiles;
+        const size_t nb = (std::max(std::max(m, rows), n) + SCAN_CHUNK - 1) / SCAN_CHUNK;
         CONAN_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         CONAN_CUDA(cudaMalloc(&X, n * R * sizeof(double)));
         CONAN_CUDA(cudaMalloc(&S, n * R * sizeof(double)));
-        CONAN_CUDA(cudaMalloc(&cell, (n + 1) * sizeof(uint32_t)));
-        CONAN_CUDA(cudaMalloc(&slot, n * sizeof(uint32_t)));
-        CONAN_CUDA(cudaMalloc(&order, n * sizeof(uint32_t)));
+        for (int b = 0; b < 2; ++b) {
+            CONAN_CUDA(cudaMalloc(&keys[b], n * sizeof(uint64_t)));
+            CONAN_CUDA(cudaMalloc(&vals[b], n * sizeof(uint32_t)));
+        }
         CONAN_CUDA(cudaMalloc(&par, n * sizeof(uint32_t)));
-        CONAN_CUDA(cudaMalloc(&count, cells * sizeof(uint32_t)));
-        CONAN_CUDA(cudaMalloc(&off, (cells + 1) * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&flag, n * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&gnum, (n + 1) * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&rowcount, rows * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&rowoff, (rows + 1) * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&bh, m * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&boff, (m + 1) * sizeof(uint32_t)));
         CONAN_CUDA(cudaMalloc(&bsum, nb * sizeof(uint32_t)));
         CONAN_CUDA(cudaMalloc(&tags, n * sizeof(unsigned long long)));
         CONAN_CUDA(cudaMalloc(&err, sizeof(int)));
         CONAN_CUDA(cudaMallocHost(&ngroups_h, 2 * sizeof(uint32_t)));
-        CONAN_CUDA(cudaMemsetAsync(count, 0, cells * sizeof(uint32_t), st));
+        CONAN_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMEM));
+        CONAN_CUDA(cudaMemsetAsync(rowcount, 0, rows * sizeof(uint32_t), st));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
         CONAN_CUDA(cudaStreamSynchronize(st));
         return CONAN_OK;
@@ -295,20 +389,24 @@ struct FofEngine {
     // Groups of the positions in Xd (device, n x R doubles); tags into tg
     // (device, n values). Enqueued on `s`; the group count is read back.
     template <int RR> int run_t(const double *Xd, unsigned long long *tg, cudaStream_t s, uint64_t *ngroups) {
-        k_fof_bin<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, g, cell, slot, count);
-        scan(count, cells, off, s);
-        k_fof_scatter<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, cell, slot, off, order, S, par);
-        k_fof_link<RR><<<blocks(n), FOF_T, 0, s>>>(S, order, off, n, g, par, err);
-        // roots into `order` and root flags into `slot` (both free after the
-        // link), group numbers into `cell`
-        k_fof_roots<<<blocks(n), FOF_T, 0, s>>>(par, n, order, slot);
-        scan(slot, n, cell, s);
-        k_fof_tags<<<blocks(n), FOF_T, 0, s>>>(order, cell, n, tg);
+        k_fof_keys<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, g, keys[0], vals[0], rowcount);
+        scan(rowcount, rows, rowoff, s);  // also clears the counts for the next run
+        const int w = radix_sort_pairs(keys, vals, n, key_bits, bh, boff, bsum, s);
+        const uint64_t *sk = keys[w];
+        const uint32_t *order = vals[w];
+        k_fof_gather<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, order, S, par);
+        FofLink a{S, sk, order, rowoff, n, g, par, err};
+        k_fof_link<RR><<<blocks(n), FOF_T, 0, s>>>(a);
+        // roots into the free value buffer, root flags, group numbers
+        uint32_t *root = vals[w ^ 1];
+        k_fof_roots<<<blocks(n), FOF_T, 0, s>>>(par, n, root, flag);
+        scan(flag, n, gnum, s);
+        k_fof_tags<<<blocks(n), FOF_T, 0, s>>>(root, gnum, n, tg);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
             return set_error(CONAN_ERR_CUDA, "fof kernel launch failed: %s", cudaGetErrorString(e));
         int herr = 0;
-        CONAN_CUDA(cudaMemcpyAsync(ngroups_h, cell + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CONAN_CUDA(cudaMemcpyAsync(ngroups_h, gnum + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         CONAN_CUDA(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
         CONAN_CUDA(cudaStreamSynchronize(s));
