@@ -126,9 +126,11 @@ __device__ inline uint32_t fof_unite(uint32_t *par, uint32_t a, uint32_t b) {
     return FOF_NONE;
 }
 
+// Key of every particle (particle order) and its rank in its row from an
+// integer counter.
 template <int R>
 __global__ void __launch_bounds__(FOF_T) k_fof_keys(const double *__restrict__ X, size_t n, FofGrid g,
-                                                    uint64_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                    uint64_t *__restrict__ keys, uint32_t *__restrict__ slot,
                                                     uint32_t *__restrict__ rowcount) {
     const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
     if (i >= n) return;
@@ -137,8 +139,109 @@ __global__ void __launch_bounds__(FOF_T) k_fof_keys(const double *__restrict__ X
     for (int k = 0; k < R; ++k) x[k] = X[i * R + k];
     uint32_t row;
     keys[i] = fof_key<R>(x, g, &row);
-    vals[i] = (uint32_t)i;
-    atomicAdd(rowcount + row, 1u);
+    slot[i] = atomicAdd(rowcount + row, 1u);
+}
+
+// Counting sort by row: every particle at its row's offset plus its rank
+// (the order inside a row is put right by the row sorts).
+__global__ void __launch_bounds__(FOF_T) k_fof_place(const uint64_t *__restrict__ kp, const uint32_t *__restrict__ slot,
+                                                     const uint32_t *__restrict__ rowoff, size_t n,
+                                                     uint64_t *__restrict__ keys, uint32_t *__restrict__ order) {
+    const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t key = kp[i];
+    const size_t t = (size_t)rowoff[key >> FOF_XB] + slot[i];
+    keys[t] = key;
+    order[t] = (uint32_t)i;
+}
+
+constexpr int FOF_BIG = 4096;  // longest row sorted in shared memory
+
+// Sort value of a sorted slot: quantised x above the particle index (unique,
+// and the order a stable sort by key from particle order would give).
+__device__ inline uint64_t fof_sortval(const uint64_t *keys, const uint32_t *order, size_t t) {
+    return ((keys[t] & FOF_XMASK) << 32) | order[t];
+}
+
+// One warp per row: rows of up to 32 particles are sorted by (x, index) with
+// a bitonic network across the lanes; longer rows are queued for
+// k_fof_rowsort_big (up to FOF_BIG) or flagged in nbig[1] (longer).
+__global__ void __launch_bounds__(256) k_fof_rowsort_small(uint64_t *__restrict__ keys, uint32_t *__restrict__ order,
+                                                           const uint32_t *__restrict__ rowoff, size_t rows,
+                                                           uint32_t *__restrict__ big, uint32_t *__restrict__ nbig) {
+    const int lane = threadIdx.x & 31;
+    const size_t nw = (size_t)gridDim.x * (256 / 32);
+    for (size_t r = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5; r < rows; r += nw) {
+        const size_t rs = rowoff[r];
+        const uint32_t m = rowoff[r + 1] - (uint32_t)rs;
+        if (m <= 1) continue;
+        if (m > 32) {
+            if (lane == 0) {
+                if (m > (uint32_t)FOF_BIG) atomicOr(nbig + 1, 1u);
+                else big[atomicAdd(nbig, 1u)] = (uint32_t)r;
+            }
+            continue;
+        }
+        uint64_t v = (uint32_t)lane < m ? fof_sortval(keys, order, rs + lane) : ~0ull;
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const uint64_t o = __shfl_xor_sync(FULL, v, j);
+                const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+                v = keep_min ? (v < o ? v : o) : (v > o ? v : o);
+            }
+        }
+        if ((uint32_t)lane < m) {
+            keys[rs + lane] = ((uint64_t)r << FOF_XB) | (v >> 32);
+            order[rs + lane] = (uint32_t)v;
+        }
+    }
+}
+
+// One CTA per queued row (33 .. FOF_BIG particles): bitonic sort in shared
+// memory over the next power of two, padded with the largest value.
+__global__ void __launch_bounds__(256) k_fof_rowsort_big(uint64_t *__restrict__ keys, uint32_t *__restrict__ order,
+                                                         const uint32_t *__restrict__ rowoff,
+                                                         const uint32_t *__restrict__ big,
+                                                         const uint32_t *__restrict__ nbig) {
+    __shared__ uint64_t sv[FOF_BIG];
+    const uint32_t nq = nbig[0];
+    for (uint32_t b = blockIdx.x; b < nq; b += gridDim.x) {
+        const uint32_t r = big[b];
+        const size_t rs = rowoff[r];
+        const uint32_t m = rowoff[r + 1] - (uint32_t)rs;
+        uint32_t P = 64;
+        while (P < m) P <<= 1;
+        for (uint32_t j = threadIdx.x; j < P; j += 256) sv[j] = j < m ? fof_sortval(keys, order, rs + j) : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t x = threadIdx.x; x < P; x += 256) {
+                    const uint32_t y = x ^ j;
+                    if (y > x) {
+                        const uint64_t a = sv[x], c = sv[y];
+                        if ((a > c) == ((x & k) == 0)) {
+                            sv[x] = c;
+                            sv[y] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t j = threadIdx.x; j < m; j += 256) {
+            const uint64_t v = sv[j];
+            keys[rs + j] = ((uint64_t)r << FOF_XB) | (v >> 32);
+            order[rs + j] = (uint32_t)v;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(FOF_T) k_fof_iota(uint32_t *__restrict__ v, size_t n) {
+    const size_t i = (size_t)blockIdx.x * FOF_T + threadIdx.x;
+    if (i < n) v[i] = (uint32_t)i;
 }
 
 template <int R>
@@ -306,18 +409,21 @@ struct FofEngine {
     uint64_t *keys[2] = {nullptr, nullptr};
     uint32_t *vals[2] = {nullptr, nullptr};
     uint32_t *par = nullptr, *rowcount = nullptr, *rowoff = nullptr, *flag = nullptr, *gnum = nullptr,
-             *bh = nullptr, *boff = nullptr, *bsum = nullptr;
+             *bh = nullptr, *boff = nullptr, *bsum = nullptr, *bigrows = nullptr, *nbig = nullptr;
     unsigned long long *tags = nullptr;
-    uint32_t *ngroups_h = nullptr;  // pinned
+    uint32_t *ngroups_h = nullptr, *nbig_h = nullptr;  // pinned
     int *err = nullptr;
+    int sort_blocks = 0;
+    bool used_radix = false;  // the last run's rows were too long for the row sorts
 
     ~FofEngine() {
         if (st) cudaStreamSynchronize(st);
         for (void *q : {(void *)X, (void *)S, (void *)keys[0], (void *)keys[1], (void *)vals[0], (void *)vals[1],
                         (void *)par, (void *)rowcount, (void *)rowoff, (void *)flag, (void *)gnum, (void *)bh,
-                        (void *)boff, (void *)bsum, (void *)tags, (void *)err})
+                        (void *)boff, (void *)bsum, (void *)tags, (void *)err, (void *)bigrows, (void *)nbig})
             cudaFree(q);
         cudaFreeHost(ngroups_h);
+        cudaFreeHost(nbig_h);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -372,6 +478,12 @@ struct FofEngine {
         CONAN_CUDA(cudaMalloc(&tags, n * sizeof(unsigned long long)));
         CONAN_CUDA(cudaMalloc(&err, sizeof(int)));
         CONAN_CUDA(cudaMallocHost(&ngroups_h, 2 * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&bigrows, std::min(rows, n / 33 + 1) * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMalloc(&nbig, 2 * sizeof(uint32_t)));
+        CONAN_CUDA(cudaMallocHost(&nbig_h, 2 * sizeof(uint32_t)));
+        int sms = 0;
+        CONAN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        sort_blocks = 8 * sms;
         CONAN_CUDA(cudaFuncSetAttribute(k_rs_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMEM));
         CONAN_CUDA(cudaMemsetAsync(rowcount, 0, rows * sizeof(uint32_t), st));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
@@ -389,16 +501,33 @@ struct FofEngine {
     // Groups of the positions in Xd (device, n x R doubles); tags into tg
     // (device, n values). Enqueued on `s`; the group count is read back.
     template <int RR> int run_t(const double *Xd, unsigned long long *tg, cudaStream_t s, uint64_t *ngroups) {
-        k_fof_keys<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, g, keys[0], vals[0], rowcount);
+        // per-particle keys into keys[1], ranks in the rows into `flag`
+        k_fof_keys<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, g, keys[1], flag, rowcount);
         scan(rowcount, rows, rowoff, s);  // also clears the counts for the next run
-        const int w = radix_sort_pairs(keys, vals, n, key_bits, bh, boff, bsum, s);
-        const uint64_t *sk = keys[w];
-        const uint32_t *order = vals[w];
+        // counting sort by row, then every row sorted by (x, index)
+        CONAN_CUDA(cudaMemsetAsync(nbig, 0, 2 * sizeof(uint32_t), s));
+        k_fof_place<<<blocks(n), FOF_T, 0, s>>>(keys[1], flag, rowoff, n, keys[0], vals[0]);
+        k_fof_rowsort_small<<<(unsigned)sort_blocks, 256, 0, s>>>(keys[0], vals[0], rowoff, rows, bigrows, nbig);
+        k_fof_rowsort_big<<<(unsigned)sort_blocks, 256, 0, s>>>(keys[0], vals[0], rowoff, bigrows, nbig);
+        CONAN_CUDA(cudaMemcpyAsync(nbig_h, nbig, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        CONAN_CUDA(cudaStreamSynchronize(s));
+        uint64_t *sk = keys[0];
+        uint32_t *order = vals[0], *root = vals[1];
+        used_radix = nbig_h[1] != 0;
+        if (used_radix) {
+            // a row longer than FOF_BIG: radix sort of (key, index) from particle order instead
+            k_fof_iota<<<blocks(n), FOF_T, 0, s>>>(vals[1], n);
+            uint64_t *kk[2] = {keys[1], keys[0]};
+            uint32_t *vv[2] = {vals[1], vals[0]};
+            const int w = radix_sort_pairs(kk, vv, n, key_bits, bh, boff, bsum, s);
+            sk = kk[w];
+            order = vv[w];
+            root = vv[w ^ 1];
+        }
         k_fof_gather<RR><<<blocks(n), FOF_T, 0, s>>>(Xd, n, order, S, par);
         FofLink a{S, sk, order, rowoff, n, g, par, err};
         k_fof_link<RR><<<blocks(n), FOF_T, 0, s>>>(a);
         // roots into the free value buffer, root flags, group numbers
-        uint32_t *root = vals[w ^ 1];
         k_fof_roots<<<blocks(n), FOF_T, 0, s>>>(par, n, root, flag);
         scan(flag, n, gnum, s);
         k_fof_tags<<<blocks(n), FOF_T, 0, s>>>(root, gnum, n, tg);

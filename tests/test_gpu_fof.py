@@ -99,3 +99,21 @@ def test_fof_rejects_bad_arguments(gpu, conan):
     for dim, L, ll in [(1, 10.0, 1.0), (4, 10.0, 1.0), (3, 0.0, 1.0), (3, 10.0, 0.0), (3, 10.0, float("nan"))]:
         with pytest.raises(conan.ConanError):
             conan.fof(X.reshape(-1)[: 10 * dim] if dim <= 3 else np.zeros((10, 4)), dim, L, ll)
+
+
+@pytest.mark.parametrize("m_row", [2_000, 10_000])
+def test_fof_long_rows(gpu, conan, oracle, m_row):
+    """One transverse cell holding a column of m_row particles along x: a row
+    sorted in shared memory (up to 4096 particles) and one that takes the
+    radix-sort path (longer)."""
+    rng = np.random.default_rng(m_row)
+    L, ll, n = 100.0, 0.8, 30_000
+    X = rng.uniform(0, L, size=(n, 3))
+    X[:m_row, 0] = rng.uniform(0, L, m_row)
+    X[:m_row, 1] = rng.uniform(50.5, 50.7, m_row)  # transverse cell (63, 25) of side 0.8
+    X[:m_row, 2] = rng.uniform(20.1, 20.3, m_row)
+    ref, ngr = oracle.fof(3, L, ll, X)
+    for _ in range(2):
+        tags, ng = conan.fof(X, 3, L, ll)
+        assert ng == ngr
+        assert np.array_equal(tags, ref)
