@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-cic", action="store_true")
     ap.add_argument("--no-fof", action="store_true")
+    ap.add_argument("--no-mesh2", action="store_true")
     return ap.parse_args()
 
 
@@ -386,8 +387,8 @@ def run_ours(args):
     hbm = peaks.get("hbm_gbs", 6650.0)
     hbm_src = "measured" if "hbm_gbs" in peaks else "fallback"
 
-    def timed_run(prec, profile=False):
-        g = cb.Gravity(3, n, f, L_BOX, precision=prec, device=dev)
+    def timed_run(prec, profile=False, mesh_f=None):
+        g = cb.Gravity(3, n, mesh_f or f, L_BOX, precision=prec, device=dev)
         s = torch.cuda.ExternalStream(g.stream_ptr())
         # warm-up: W steps from the initial conditions (plans, graphs, caches)
         g.run(phi, A0, DA, args.warmup)
@@ -457,6 +458,42 @@ def run_ours(args):
         err = float(np.max(np.abs(P32[m] - P64[m]) / P64[m]))
         fp64 = {"value": world * Np * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
                 "pk_max_rel_err_fp32_vs_fp64": err, "fp32_speedup": ms64 / ms32}
+
+    # the throughput box's finer-mesh variant (2N per side: 1024^3 cells at 512^3
+    # particles): FP32 and FP64 runs of the same K steps, P(k) error between them
+    mesh2 = None
+    if not args.no_mesh2 and f == 1:
+        Nc2 = (2 * n) ** 3
+        g2, ms2, _, _ = timed_run("fp32", mesh_f=2)
+        ms2 = max_over_ranks(ms2, dist)
+        _, P2, c2 = g2.power_spectrum()
+        g2.close()
+        mesh2 = {"workload": workload_name(mbits, 2), "ms_per_step": ms2 / args.steps,
+                 "value": world * Np * args.steps / (ms2 * 1e-3), "unit": "particle-steps/s",
+                 "step_roofline_frac": (60 * Np + 24 * Nc2) * args.steps / (ms2 * 1e-3) / 1e9 / hbm}
+        if not args.no_fp64:
+            g2d, ms2d, _, _ = timed_run("fp64", mesh_f=2)
+            ms2d = max_over_ranks(ms2d, dist)
+            _, P2d, _ = g2d.power_spectrum()
+            g2d.close()
+            m2 = (c2 > 0) & (np.arange(len(c2)) > 0)
+            mesh2["fp64_ms_per_step"] = ms2d / args.steps
+            mesh2["pk_max_rel_err_fp32_vs_fp64"] = float(np.max(np.abs(P2[m2] - P2d[m2]) / P2d[m2]))
+
+    # the host link of this box (one pinned 1 GiB copy each way, CUDA events):
+    # the end-to-end number below moves 7.5 GB across it
+    link = {}
+    hb = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()
+    db = torch.empty(1 << 30, dtype=torch.uint8, device=f"cuda:{dev}")
+    for name, dst, src in (("h2d_gbs", db, hb), ("d2h_gbs", hb, db)):
+        dst.copy_(src, non_blocking=True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        link[name] = (1 << 30) / (e0.elapsed_time(e1) * 1e-3) / 1e9
+    del hb, db
 
     # end-to-end through the C ABI with host buffers: phi in, X and P out
     ph = torch.from_numpy(phi).pin_memory().numpy()
@@ -560,6 +597,7 @@ def run_ours(args):
             "kernels": kernels,
             "gpu_launches": launches,
             "fp64_gpu": fp64,
+            "mesh_2n": mesh2,
             "adjoint": adjoint,
             "ensemble": ensemble,
             "cic": cic,
@@ -567,7 +605,8 @@ def run_ours(args):
             "e2e": {"value": world * Np * args.steps / e2e_s, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": phi.nbytes / args.steps,
                     "d2h_bytes_per_step": (Xh.nbytes + Ph.nbytes) / args.steps,
-                    "what": "conan_pm_run (potential upload, Zel'dovich init, K steps) + conan_pm_get_state"},
+                    "what": "conan_pm_run (potential upload, Zel'dovich init, K steps) + conan_pm_get_state",
+                    "seconds": e2e_s, "host_link": link},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }
