@@ -157,7 +157,14 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_TRY(alloc(&err, 1));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
         CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
-        if (sizeof(T) == 4 && (lag_try<0>() || lag_try<1>() || lag_try<2>())) {
+        bool lag = sizeof(T) == 4 && (lag_try<0>() || lag_try<1>() || lag_try<2>());
+        // On fine meshes (f >= 2) a window that fits shared memory only fits
+        // a small tile and holds many cells per particle, each of which gets
+        // about one corner: clearing and flushing it costs more than the
+        // atomics it saves. Deposit directly from the largest tile then.
+        if (sizeof(T) == 4 && (!lag || (double)lwin.cells > LAG_WINDOW_CELLS_PER_PARTICLE * lag_particles()))
+            lag = lag_try<0>(true) || lag_try<1>(true) || lag_try<2>(true);
+        if (lag) {
             CONAN_TRY(alloc(&lacc, mf.cells));
             CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st));
             dep_variant = DEP_LAG;
@@ -204,14 +211,23 @@ template <typename T, int R> struct PM : PMBase {
 
     bool lag_on() const { return sizeof(T) == 4 && dep_variant == DEP_LAG && lag_v >= 0 && lacc; }
 
-    template <int V> bool lag_try() {
+    template <int V> static constexpr double lag_tile_particles() {
+        return (double)LagTile<R, V>::LX * LagTile<R, V>::LY * LagTile<R, V>::LZ;
+    }
+    double lag_particles() const {
+        return lag_v == 0 ? lag_tile_particles<0>() : lag_v == 1 ? lag_tile_particles<1>() : lag_tile_particles<2>();
+    }
+
+    // direct: a window of two cells per axis, so that (nearly) every corner
+    // goes straight to the accumulator mesh with one integer atomic.
+    template <int V> bool lag_try(bool direct = false) {
         typedef LagTile<R, V> L;
         const int n = mm.n;
         if (n < L::LX || (R >= 2 && n < L::LY) || (R == 3 && n < L::LZ)) return false;
         LagWin w{};
-        w.w[0] = L::LX * prm.f + L::M;
-        w.w[1] = R >= 2 ? L::LY * prm.f + L::M : 1;
-        w.w[2] = R == 3 ? L::LZ * prm.f + L::M : 1;
+        w.w[0] = direct ? 2 : L::LX * prm.f + L::M;
+        w.w[1] = R >= 2 ? (direct ? 2 : L::LY * prm.f + L::M) : 1;
+        w.w[2] = R == 3 ? (direct ? 2 : L::LZ * prm.f + L::M) : 1;
         w.cells = (w.w[0] * w.w[1] * w.w[2] + 3) & ~3;
         size_t sh = (size_t)w.cells * 2 * sizeof(uint32_t);
         if (sh > 112 * 1024) return false;

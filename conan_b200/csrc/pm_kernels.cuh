@@ -751,6 +751,12 @@ struct LagWin {
 // Lattice tile (LX x LY x LZ particles), threads and window margin M (cells
 // beyond the tile's own f*L cells, split over both sides) of variant V.
 constexpr int LAG_VARIANTS = 3;
+// Window cells per particle of a tile above which the deposit goes to the
+// accumulator mesh directly (fine meshes); a compile-time tunable.
+#ifndef LAG_WINDOW_CELLS_PER_PARTICLE
+#define LAG_WINDOW_CELLS_PER_PARTICLE 12.0
+#endif
+
 template <int R, int V> struct LagTile;
 template <> struct LagTile<3, 0> { static constexpr int LX = 32, LY = 8, LZ = 8, THREADS = 512, M = 8; };
 template <> struct LagTile<3, 1> { static constexpr int LX = 16, LY = 8, LZ = 8, THREADS = 256, M = 8; };
