@@ -218,9 +218,9 @@ def fof_bench(cb, Xh, n, dev, steps, reps=3):
                     "d2h_bytes": tags_h.nbytes, "what": "conan_fof_run: host positions in, host tags out"}}
 
 
-def fof_tool_vs_reference(cb, n_sample=64, max_seconds=60.0):
-    """The whole `fof` tool (snapshot file in, text file out) on a 64^3 box
-    with the throughput box's spacing (L = 62.5 Mpc/h) run to a = 1 on the GPU:
+def fof_tool_vs_reference(cb, n_sample=128, max_seconds=60.0):
+    """The whole `fof` tool (snapshot file in, text file out) on a 128^3 box
+    with the throughput box's spacing (L = 125 Mpc/h) run to a = 1 on the GPU:
     the reference's binary (oracle/_ref/conan_ref, single-threaded kd-tree)
     against this build's `conan fof`, same file and options; the two text
     outputs must agree after the header and history."""
@@ -536,7 +536,7 @@ def run_ours(args):
     if rank == 0 and not args.no_fof:
         fof = fof_bench(cb, Xh, n, dev, args.steps)
         if not args.no_cpu:
-            fof["tool_64"] = fof_tool_vs_reference(cb)
+            fof["tool_128"] = fof_tool_vs_reference(cb)
 
     adjoint = None
     if not args.no_adjoint and rank == 0:
