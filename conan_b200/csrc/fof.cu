@@ -12,8 +12,12 @@
 //            y and z) on a grid of cells no smaller than the linking length,
 //            wrapped coordinates -- and its wrapped x quantised to 2^16
 //            steps, as one 64-bit key; an integer count per row;
-//   sort     stable radix sort of (key, particle index) (radix.cuh): rows in
-//            order, x ascending inside a row; row offsets from the counts;
+//   sort     counting sort by row (offsets from the counts), then every row
+//            sorted by (x, particle index): across the lanes of a warp up to
+//            32 particles, in shared memory up to 4096; a longer row sends
+//            the whole array through a stable radix sort of (key, particle
+//            index) instead (radix.cuh). Either way: rows in order, x
+//            ascending inside a row, ties in particle order;
 //   gather   coordinates (one array per axis) in sorted order;
 //   link     one thread per sorted particle tests, in its own row, the
 //            particles ahead of it in cyclic x order within the linking
