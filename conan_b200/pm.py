@@ -166,6 +166,15 @@ class FoF:
             self.h = None
 
     def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the module's globals may be gone
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
         self.close()
 
 
