@@ -73,7 +73,7 @@ template <int R, int V> int window_of(int n, int f, LagWin *w, size_t *smem) {
     x.w[1] = R >= 2 ? L::LY * f + L::M : 1;
     x.w[2] = R == 3 ? L::LZ * f + L::M : 1;
     x.cells = (x.w[0] * x.w[1] * x.w[2] + 3) & ~3;
-    size_t sh = (size_t)x.cells * 2 * sizeof(uint32_t);
+    size_t sh = (size_t)x.cells * LAG_PLANES * sizeof(uint32_t);
     if (sh > 112 * 1024) return 0;
     *w = x;
     *smem = sh;

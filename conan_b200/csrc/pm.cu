@@ -229,7 +229,7 @@ template <typename T, int R> struct PM : PMBase {
         w.w[1] = R >= 2 ? (direct ? 2 : L::LY * prm.f + L::M) : 1;
         w.w[2] = R == 3 ? (direct ? 2 : L::LZ * prm.f + L::M) : 1;
         w.cells = (w.w[0] * w.w[1] * w.w[2] + 3) & ~3;
-        size_t sh = (size_t)w.cells * 2 * sizeof(uint32_t);
+        size_t sh = (size_t)w.cells * LAG_PLANES * sizeof(uint32_t);
         if (sh > 112 * 1024) return false;
         if constexpr (sizeof(T) == 4) {  // set once here, outside any stream capture
             auto kern = k_deposit_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;

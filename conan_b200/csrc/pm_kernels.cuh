@@ -751,6 +751,12 @@ struct LagWin {
 // Lattice tile (LX x LY x LZ particles), threads and window margin M (cells
 // beyond the tile's own f*L cells, split over both sides) of variant V.
 constexpr int LAG_VARIANTS = 3;
+// 32-bit planes of a window cell: 2 keeps the carry in shared memory, 1
+// sends it to the accumulator mesh; a compile-time tunable.
+#ifndef LAG_PLANES
+#define LAG_PLANES 2
+#endif
+
 // Window cells per particle of a tile above which the deposit goes to the
 // accumulator mesh directly (fine meshes); a compile-time tunable.
 #ifndef LAG_WINDOW_CELLS_PER_PARTICLE
@@ -867,7 +873,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     }
     if constexpr (STAGED) __syncthreads();  // staged particles are read before the window reuses the memory
     uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
-    for (int c = threadIdx.x; c < cells / 2; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    for (int c = threadIdx.x; c < cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     if (threadIdx.x < R) {
         const int k = threadIdx.x;
@@ -923,8 +929,20 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                Slot<float>::add(lag_sh, base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1, v,
-                                 cells);
+                const int wc = base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1;
+                if constexpr (LAG_PLANES == 2) {
+                    Slot<float>::add(lag_sh, wc, v, cells);
+                } else if (v) {
+                    // one plane: a carry out of the 32-bit cell goes to the
+                    // accumulator mesh directly (rare: over 2^9 particles' weight)
+                    const uint32_t old = atomicAdd(lag_sh + wc, v);
+                    if (old + v < old) {
+                        size_t g = (size_t)((u[0] + (b & 1)) & mask);
+                        if (R >= 2) g |= (size_t)((u[1] + ((b >> 1) & 1)) & mask) << m.shift;
+                        if (R == 3) g |= (size_t)((u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+                        atomicAdd(acc + cb + g, 1ull << 32);
+                    }
+                }
             }
         } else {
 #pragma unroll
@@ -948,7 +966,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     const int s0 = THREADS % E0, s1 = (THREADS / E0) % E1, s2 = THREADS / (E0 * E1);
     for (int c = threadIdx.x; c < ecells; c += THREADS) {
         const int wc = (l2 * W1 + l1) * W0 + l0;
-        uint32_t a = lag_sh[wc], b = lag_sh[cells + wc];
+        uint32_t a = lag_sh[wc], b = LAG_PLANES == 2 ? lag_sh[cells + wc] : 0u;
         if (a | b) {
             size_t g = (size_t)((o0 + l0) & mask);
             if (R >= 2) g |= (size_t)((o1 + l1) & mask) << m.shift;
