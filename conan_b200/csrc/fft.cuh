@@ -31,6 +31,25 @@ struct FFTPair {
         work_bytes = w1 > w2 ? w1 : w2;
         return CONAN_OK;
     }
+    // 2D transforms of every z plane (3D meshes): the same half-spectrum
+    // layout as the 3D pair with z left in real space.
+    int create_planes(const Mesh &m, bool is_double, int batch) {
+        dbl = is_double;
+        int n[2] = {m.n, m.n};
+        long long real_dist = (long long)m.n * m.n, cplx_dist = (long long)m.n * m.nh;
+        const int planes = batch * m.n;
+        size_t w1 = 0, w2 = 0;
+        CONAN_CUFFT(cufftCreate(&r2c));
+        CONAN_CUFFT(cufftCreate(&c2r));
+        CONAN_CUFFT(cufftSetAutoAllocation(r2c, 0));
+        CONAN_CUFFT(cufftSetAutoAllocation(c2r, 0));
+        CONAN_CUFFT(cufftMakePlanMany(r2c, 2, n, nullptr, 1, (int)real_dist, nullptr, 1, (int)cplx_dist,
+                                      dbl ? CUFFT_D2Z : CUFFT_R2C, planes, &w1));
+        CONAN_CUFFT(cufftMakePlanMany(c2r, 2, n, nullptr, 1, (int)cplx_dist, nullptr, 1, (int)real_dist,
+                                      dbl ? CUFFT_Z2D : CUFFT_C2R, planes, &w2));
+        work_bytes = w1 > w2 ? w1 : w2;
+        return CONAN_OK;
+    }
     int bind(void *work, cudaStream_t s) {
         CONAN_CUFFT(cufftSetWorkArea(r2c, work));
         CONAN_CUFFT(cufftSetWorkArea(c2r, work));

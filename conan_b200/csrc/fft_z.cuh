@@ -1,0 +1,215 @@
+// fft_z.cuh -- the z direction of the Poisson solve's 3D transform, done in
+// shared memory with the Green's function multiply in between.
+//
+// With cuFFT's 2D R2C over every z plane of the density, the half spectrum of
+// one member is (z, ky, kx) with kx fastest: z still in real space. One CTA
+// takes TX consecutive kx columns of one ky row, i.e. TX complex lines of n
+// values along z (stride n * nh), and runs
+//   forward complex FFT along z (natural order out)
+//   spec *= gs / |k|^2, DC = 0 (the multiply of k_green: same formula)
+//   inverse complex FFT along z (unnormalised)
+// in shared memory, so the spectrum crosses HBM once between the forward and
+// the inverse 2D transforms instead of three times (3D transforms' z passes
+// and the multiply). The 2D C2R per plane then gives phi.
+//
+// The FFT is the Stockham self-sorting formulation (Govindaraju et al.,
+// "High performance discrete Fourier transforms on graphics processors",
+// SC 2008): stage with sub-length Ns and radix R reads x[j + r N/R], applies
+// the twiddles exp(-+2 pi i (j mod Ns) r / (Ns R)), a radix-R DFT in
+// registers, and writes x[(j / Ns) Ns R + (j mod Ns) + r Ns]. Radix 8
+// stages, then one radix-2 or radix-4 stage for n = 8^a * {1, 2, 4}. Each
+// stage reads all its inputs, synchronises, and writes in place. Twiddles
+// come from a table of exp(-2 pi i k / n) computed in double on the host.
+#pragma once
+
+#include "common.cuh"
+
+namespace conan {
+
+// Lines per CTA and threads per CTA for an n-point z transform: n / 8
+// threads per line.
+template <int N> struct ZTile {
+    static constexpr int TX = N >= 256 ? 8 : 2048 / N;
+    static constexpr int LT = N / 8;  // threads per line
+    static constexpr int THREADS = TX * LT;
+    static constexpr size_t SMEM = (size_t)TX * N * sizeof(float2) + (size_t)N * sizeof(float2);
+};
+
+__device__ inline float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ inline float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ inline float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// times -i (forward) or +i (inverse)
+template <bool INV> __device__ inline float2 cmul_mi(float2 a) {
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// In-register DFT of RAD = 2, 4 or 8 values, natural order in and out
+// (radix-2 decimation in frequency, outputs unscrambled by bit reversal).
+template <int RAD, bool INV> __device__ inline void dft_small(float2 *v) {
+    if constexpr (RAD == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (RAD == 4) {
+        const float2 a0 = cadd(v[0], v[2]), a2 = csub(v[0], v[2]);
+        const float2 a1 = cadd(v[1], v[3]), a3 = cmul_mi<INV>(csub(v[1], v[3]));
+        v[0] = cadd(a0, a1);
+        v[2] = csub(a0, a1);
+        v[1] = cadd(a2, a3);
+        v[3] = csub(a2, a3);
+    } else {
+        const float h = 0.70710678118654752440f;  // 1 / sqrt(2)
+        float2 a[8];
+        a[0] = cadd(v[0], v[4]);
+        a[1] = cadd(v[1], v[5]);
+        a[2] = cadd(v[2], v[6]);
+        a[3] = cadd(v[3], v[7]);
+        a[4] = csub(v[0], v[4]);
+        const float2 d1 = csub(v[1], v[5]), d3 = csub(v[3], v[7]);
+        // d1 * W8, d2 * W8^2, d3 * W8^3 with W8 = exp(-+ i pi / 4)
+        a[5] = INV ? make_float2((d1.x - d1.y) * h, (d1.x + d1.y) * h) : make_float2((d1.x + d1.y) * h, (d1.y - d1.x) * h);
+        a[6] = cmul_mi<INV>(csub(v[2], v[6]));
+        a[7] = INV ? make_float2(-(d3.x + d3.y) * h, (d3.x - d3.y) * h) : make_float2((d3.y - d3.x) * h, -(d3.x + d3.y) * h);
+        float2 b[8];
+        b[0] = cadd(a[0], a[2]);
+        b[1] = cadd(a[1], a[3]);
+        b[2] = csub(a[0], a[2]);
+        b[3] = cmul_mi<INV>(csub(a[1], a[3]));
+        b[4] = cadd(a[4], a[6]);
+        b[5] = cadd(a[5], a[7]);
+        b[6] = csub(a[4], a[6]);
+        b[7] = cmul_mi<INV>(csub(a[5], a[7]));
+        v[0] = cadd(b[0], b[1]);
+        v[4] = csub(b[0], b[1]);
+        v[2] = cadd(b[2], b[3]);
+        v[6] = csub(b[2], b[3]);
+        v[1] = cadd(b[4], b[5]);
+        v[5] = csub(b[4], b[5]);
+        v[3] = cadd(b[6], b[7]);
+        v[7] = csub(b[6], b[7]);
+    }
+}
+
+// Where a stage reads from and writes to: shared memory (value index e of
+// line l at buf[e * TX + l]) or the spectrum in global memory (value e of line
+// l at g[e * zs + l], lines at or beyond `valid` neither read nor written).
+struct ZIO {
+    float2 *buf;
+    float2 *g;
+    size_t zs;
+    int valid;
+};
+
+// Green's function of the value at z index e of line l: the multiply of
+// k_green with kz = wave(e).
+struct ZGreen {
+    long long kyy;  // ky^2 of the row
+    int kx0;        // kx of line 0
+    int n;
+    float gs;
+    __device__ inline float operator()(int e, int l) const {
+        const int kz = e > n / 2 ? e - n : e;
+        const long long k2 = (long long)(kx0 + l) * (kx0 + l) + kyy + (long long)kz * kz;
+        return k2 > 0 ? gs / (float)k2 : 0.0f;
+    }
+};
+
+// One Stockham stage of radix RAD with sub-length Ns. IN_G / OUT_G: read from
+// / write to global memory instead of shared memory; GREEN: multiply the
+// inputs by the Green's function first.
+template <int N, int RAD, bool INV, bool IN_G, bool OUT_G, bool GREEN>
+__device__ inline void zstage(const ZIO &io, int Ns, const float2 *tw, const ZGreen &gf) {
+    constexpr int TX = ZTile<N>::TX, LT = ZTile<N>::LT;
+    constexpr int NB = N / RAD;  // butterflies per line
+    constexpr int Q = NB / LT;   // butterflies per thread
+    const int l = (int)threadIdx.x % TX, j0 = (int)threadIdx.x / TX;
+    float2 v[Q][RAD];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int j = j0 + q * LT;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) {
+            const int e = j + r * NB;
+            float2 x;
+            if constexpr (IN_G) x = l < io.valid ? io.g[(size_t)e * io.zs + l] : make_float2(0.f, 0.f);
+            else x = io.buf[e * TX + l];
+            if constexpr (GREEN) {
+                const float g = gf(e, l);
+                x.x *= g;
+                x.y *= g;
+            }
+            v[q][r] = x;
+        }
+    }
+    if constexpr (!IN_G) __syncthreads();  // every input read before any output lands in place
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int j = j0 + q * LT, k = j % Ns;
+        const int step = N / (Ns * RAD);
+#pragma unroll
+        for (int r = 1; r < RAD; ++r) {
+            float2 w = tw[(k * r * step) & (N - 1)];
+            if (INV) w.y = -w.y;
+            v[q][r] = cmul(v[q][r], w);
+        }
+        dft_small<RAD, INV>(v[q]);
+        const int base = (j / Ns) * Ns * RAD + k;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) {
+            const int e = base + r * Ns;
+            if constexpr (OUT_G) {
+                if (l < io.valid) io.g[(size_t)e * io.zs + l] = v[q][r];
+            } else {
+                io.buf[e * TX + l] = v[q][r];
+            }
+        }
+    }
+    if constexpr (!OUT_G) __syncthreads();
+}
+
+// Radix of stage s of an n-point transform: 8 while 8 divides the rest.
+template <int N> struct ZRadix {
+    static constexpr int S8 = N >= 512 ? 3 : 2;  // radix-8 stages (64..1024 points)
+    static constexpr int REST = N / (S8 == 3 ? 512 : 64);  // 1, 2 or 4
+};
+
+// Forward z FFT, Green multiply, inverse z FFT for TX columns of one row.
+// Grid: (ceil(nh / TX), n rows ky, members). spec: the members' half spectra
+// after the 2D transforms of every z plane.
+template <int N>
+__global__ void __launch_bounds__(ZTile<N>::THREADS) k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
+                                                                   const float2 *__restrict__ twid) {
+    extern __shared__ __align__(16) float2 zsh[];
+    constexpr int TX = ZTile<N>::TX;
+    float2 *tw = zsh + TX * N;
+    for (int i = threadIdx.x; i < N; i += ZTile<N>::THREADS) tw[i] = twid[i];
+    __syncthreads();
+    const int kx0 = (int)blockIdx.x * TX, ky = (int)blockIdx.y;
+    const size_t zs = (size_t)m.n * m.nh;
+    ZIO io{zsh, spec + (size_t)blockIdx.z * m.mspec + (size_t)ky * m.nh + kx0, zs, m.nh - kx0};
+    const int wy = wave_index(ky, m.n);
+    const ZGreen gf{(long long)wy * wy, kx0, m.n, gs};
+    constexpr int S8 = ZRadix<N>::S8, REST = ZRadix<N>::REST;
+    // forward: radix-8 stages (the first from global memory), then the rest
+    int Ns = 1;
+    zstage<N, 8, false, true, false, false>(io, Ns, tw, gf);
+    Ns *= 8;
+#pragma unroll
+    for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, 8, false, false, false, false>(io, Ns, tw, gf);
+    if constexpr (REST > 1) zstage<N, REST, false, false, false, false>(io, Ns, tw, gf);
+    // inverse, the Green's function applied as the first stage reads
+    Ns = 1;
+    zstage<N, 8, true, false, false, true>(io, Ns, tw, gf);
+    Ns *= 8;
+    if constexpr (REST > 1) {
+#pragma unroll
+        for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, 8, true, false, false, false>(io, Ns, tw, gf);
+        zstage<N, REST, true, false, true, false>(io, Ns, tw, gf);
+    } else {
+#pragma unroll
+        for (int s = 1; s < S8 - 1; ++s, Ns *= 8) zstage<N, 8, true, false, false, false>(io, Ns, tw, gf);
+        zstage<N, 8, true, false, true, false>(io, Ns, tw, gf);
+    }
+}
+
+}  // namespace conan

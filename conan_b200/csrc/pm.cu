@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "fft_z.cuh"
 #include "ic.cuh"
 #include "pm.cuh"
 
@@ -89,6 +90,11 @@ template <typename T, int R> struct PM : PMBase {
     size_t xfer_n = 0;
     void *work = nullptr;
     FFTPair fft;
+    // FP32 3D FD4 meshes of 64..1024 cells per side: the Poisson solve as 2D
+    // transforms of the z planes around the shared-memory z pass (fft_z.cuh)
+    FFTPair fft2;
+    float2 *ztw = nullptr;  // exp(-2 pi i k / n), k < n
+    bool zpass = false;
     cudaStream_t st = nullptr;
     Profiler prof;
     std::vector<void *> allocs;
@@ -101,6 +107,7 @@ template <typename T, int R> struct PM : PMBase {
     ~PM() override {
         if (st) cudaStreamSynchronize(st);
         fft.destroy();
+        fft2.destroy();
         for (void *p : allocs) cudaFree(p);
         if (st) cudaStreamDestroy(st);
     }
@@ -171,8 +178,16 @@ template <typename T, int R> struct PM : PMBase {
             CONAN_TRY(tma_setup());
         }
         CONAN_TRY(fft.create(mf, sizeof(T) == 8, batch));
-        CONAN_TRY(alloc((char **)&work, fft.work_bytes));
+        size_t wbytes = fft.work_bytes;
+        if (sizeof(T) == 4 && R == 3 && p.gradient == CONAN_GRAD_FD4 && mf.n >= 64 && mf.n <= 1024) {
+            CONAN_TRY(fft2.create_planes(mf, false, batch));
+            CONAN_TRY(zpass_setup());
+            wbytes = std::max(wbytes, fft2.work_bytes);
+            zpass = true;
+        }
+        CONAN_TRY(alloc((char **)&work, wbytes));
         CONAN_TRY(fft.bind(work, st));
+        if (zpass) CONAN_TRY(fft2.bind(work, st));
         CONAN_CUDA(cudaStreamSynchronize(st));
         return CONAN_OK;
     }
@@ -442,9 +457,62 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
+    int zpass_setup() {
+        std::vector<float2> w((size_t)mf.n);
+        for (int k = 0; k < mf.n; ++k) {
+            const double a = -2.0 * M_PI * (double)k / (double)mf.n;
+            w[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
+        CONAN_TRY(alloc(&ztw, (size_t)mf.n));
+        CONAN_CUDA(cudaMemcpy(ztw, w.data(), w.size() * sizeof(float2), cudaMemcpyHostToDevice));
+        switch (mf.n) {
+            case 64: return zpass_attr<64>();
+            case 128: return zpass_attr<128>();
+            case 256: return zpass_attr<256>();
+            case 512: return zpass_attr<512>();
+            default: return zpass_attr<1024>();
+        }
+    }
+    template <int N> int zpass_attr() {
+        CONAN_CUDA(cudaFuncSetAttribute(k_zpass_green<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)ZTile<N>::SMEM));
+        return CONAN_OK;
+    }
+    template <int N> void zpass_launch(float gs) {
+        const dim3 grid((unsigned)((mf.nh + ZTile<N>::TX - 1) / ZTile<N>::TX), (unsigned)mf.n, (unsigned)mf.batch);
+        k_zpass_green<N><<<grid, ZTile<N>::THREADS, ZTile<N>::SMEM, st>>>(reinterpret_cast<float2 *>(spec), mf, gs,
+                                                                         ztw);
+    }
+    // z FFT, Green multiply and inverse z FFT of the plane spectra (FP32)
+    int green_z(double gs) {
+        if constexpr (sizeof(T) == 4) {
+            switch (mf.n) {
+                case 64: CONAN_TIMED(prof, "green", st, zpass_launch<64>((float)gs)); break;
+                case 128: CONAN_TIMED(prof, "green", st, zpass_launch<128>((float)gs)); break;
+                case 256: CONAN_TIMED(prof, "green", st, zpass_launch<256>((float)gs)); break;
+                case 512: CONAN_TIMED(prof, "green", st, zpass_launch<512>((float)gs)); break;
+                default: CONAN_TIMED(prof, "green", st, zpass_launch<1024>((float)gs)); break;
+            }
+            return CONAN_OK;
+        } else {
+            return set_error(CONAN_ERR_UNSUPPORTED, "the z pass is FP32 only");
+        }
+    }
+
     int poisson(double a) {
         // per-member normalisation: 1 / (cells of one box)
         double gs = -G / (a * (double)((size_t)1 << mf.cshift)) * std::pow(prm.size / (2 * M_PI), 2);
+        if (zpass) {
+            // 2D R2C of every z plane, z pass with the Green multiply, 2D C2R
+            if constexpr (sizeof(T) == 4) {
+                CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft2.forward(mesh, spec)));
+                CONAN_TRY(green_z(gs));
+                CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft2.inverse(spec, mesh)));
+                CONAN_TRY(fd_gradient(mesh, grad));
+                mesh_holds = 2;
+                return CONAN_OK;
+            }
+        }
         unsigned gb = (unsigned)((mf.spec + 255) / 256);
         CONAN_TIMED(prof, "fft_r2c", st, CONAN_TRY(fft.forward(mesh, spec)));
         CONAN_TRY(green(spec, gs));

@@ -134,7 +134,7 @@ def test_deposit_modes_give_identical_runs(gpu, conan, oracle):
     g.close()
 
 
-@pytest.mark.parametrize("dim,Nm,f", [(2, 64, 1), (3, 32, 1), (3, 16, 2), (1, 64, 2)])
+@pytest.mark.parametrize("dim,Nm,f", [(2, 64, 1), (3, 32, 1), (3, 16, 2), (1, 64, 2), (3, 64, 1), (3, 32, 2)])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 3e-4)])
 def test_kick_and_drift_match_reference(gpu, conan, oracle, dim, Nm, f, prec, tol):
     L = 50.0
@@ -276,3 +276,20 @@ def test_cic_tool_matches_oracle(gpu, conan, oracle, dim, Nm, f, s):
     total = Nm ** dim if s == 1 else (Nm * f) ** dim
     assert abs(got.sum() - total) < 1e-9 * total
     assert np.array_equal(got, conan.cic(X, dim, Nm, L, f=f, sub_sample=s))  # order-independent sums
+
+
+@pytest.mark.parametrize("Nm,f", [(64, 1), (128, 1), (64, 2), (256, 1)])
+def test_plane_transforms_and_z_pass_give_the_3d_potential(gpu, conan, Nm, f):
+    """FP32 3D meshes of 64..1024 cells solve Poisson as 2D transforms of the
+    z planes around the shared-memory z pass; the potential equals the FP64
+    solve (3D transforms) on the same particles to FP32 rounding."""
+    L = 100.0
+    X, Pm = _particles(3, Nm, f, L, 2.0, 9)
+    phis = {}
+    for prec in ("fp32", "fp64"):
+        g = conan.Gravity(3, Nm, f, L, precision=prec)
+        g.set_state(X, Pm, 0.4, 0.4)
+        g.kick(0.4, 0.01)
+        phis[prec] = g.potential()
+        g.close()
+    assert rel(phis["fp32"], phis["fp64"]) < 2e-5
