@@ -146,11 +146,13 @@ __device__ inline void zstage(const ZIO &io, int Ns, const float2 *tw, const ZGr
     for (int q = 0; q < Q; ++q) {
         const int j = j0 + q * LT, k = j % Ns;
         const int step = N / (Ns * RAD);
+        if (Ns > 1) {  // the first stage's twiddles are all exactly 1
 #pragma unroll
-        for (int r = 1; r < RAD; ++r) {
-            float2 w = tw[(k * r * step) & (N - 1)];
-            if (INV) w.y = -w.y;
-            v[q][r] = cmul(v[q][r], w);
+            for (int r = 1; r < RAD; ++r) {
+                float2 w = tw[(k * r * step) & (N - 1)];
+                if (INV) w.y = -w.y;
+                v[q][r] = cmul(v[q][r], w);
+            }
         }
         dft_small<RAD, INV>(v[q]);
         const int base = (j / Ns) * Ns * RAD + k;
@@ -176,8 +178,12 @@ template <int N> struct ZRadix {
 // Forward z FFT, Green multiply, inverse z FFT for TX columns of one row.
 // Grid: (ceil(nh / TX), n rows ky, members). spec: the members' half spectra
 // after the 2D transforms of every z plane.
+#ifndef ZPASS_MIN_BLOCKS
+#define ZPASS_MIN_BLOCKS 3  // resident CTAs per SM the register budget must allow (measured: 0.45 against 0.51 ms with 1 at 512^3)
+#endif
+
 template <int N>
-__global__ void __launch_bounds__(ZTile<N>::THREADS) k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
+__global__ void __launch_bounds__(ZTile<N>::THREADS, ZPASS_MIN_BLOCKS) k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
                                                                    const float2 *__restrict__ twid) {
     extern __shared__ __align__(16) float2 zsh[];
     constexpr int TX = ZTile<N>::TX;
