@@ -27,7 +27,8 @@
 namespace conan {
 
 // Lines per CTA and threads per CTA for an n-point z transform: n / 8
-// threads per line.
+// threads per line. (At n = 1024, 4 lines per CTA instead of 8 measured
+// slower: 31.0 against 30.0 ms per step of the 1024^3-mesh run.)
 template <int N> struct ZTile {
     static constexpr int TX = N >= 256 ? 8 : 2048 / N;
     static constexpr int LT = N / 8;  // threads per line

@@ -278,7 +278,7 @@ def test_cic_tool_matches_oracle(gpu, conan, oracle, dim, Nm, f, s):
     assert np.array_equal(got, conan.cic(X, dim, Nm, L, f=f, sub_sample=s))  # order-independent sums
 
 
-@pytest.mark.parametrize("Nm,f", [(64, 1), (128, 1), (64, 2), (256, 1)])
+@pytest.mark.parametrize("Nm,f", [(64, 1), (128, 1), (64, 2), (256, 1), (64, 8), (64, 16)])
 def test_plane_transforms_and_z_pass_give_the_3d_potential(gpu, conan, Nm, f):
     """FP32 3D meshes of 64..1024 cells solve Poisson as 2D transforms of the
     z planes around the shared-memory z pass; the potential equals the FP64
