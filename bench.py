@@ -418,6 +418,19 @@ def run_ours(args):
     # kernels only: cuFFT launches count as library work, the accumulator clear is a memset
     launches = sum(v[0] for k, v in prof.items() if not k.startswith("fft") and k != "deposit_clear")
     gp.close()
+    # The headline and the profile are runs of the same K steps. A headline
+    # far slower than the sum of the profiled kernels was disturbed (clocks,
+    # another job on the box): it is timed once more, and both are reported.
+    # The decision is taken over all ranks so that every rank runs the same
+    # collectives.
+    prof_ms = sum(v[1] for v in prof.values())
+    remeasured = None
+    if max_over_ranks(1.0 if prof_ms > 0 and ms32 > 1.15 * prof_ms else 0.0, dist) > 0:
+        g2, ms_again, clocks_again, _ = timed_run("fp32")
+        g2.close()
+        remeasured = {"first_ms_per_step": ms32 / args.steps, "profile_ms_per_step": prof_ms / args.steps,
+                      "first_clocks": clocks}
+        ms32, clocks = max_over_ranks(ms_again, dist), clocks_again
     dom = max((k for k in prof if algorithmic_bytes(k, Np, Nc, False)), key=lambda k: prof[k][1])
     dom_ms = prof[dom][1] / prof[dom][0]
     ab = algorithmic_bytes(dom, Np, Nc, False)
@@ -609,6 +622,7 @@ def run_ours(args):
                     "seconds": e2e_s, "host_link": link},
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "remeasured": remeasured,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
