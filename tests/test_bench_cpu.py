@@ -1,0 +1,50 @@
+"""The measurement plumbing of bench.py that needs no GPU: the algorithmic
+bytes of each kernel, the committed DRAM traffic it reports beside them, and
+the JSON line of the reference arm (the reference's own CPU code)."""
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+@pytest.fixture(scope="module")
+def bench():
+    sys.path.insert(0, str(ROOT))
+    import bench as b
+    return b
+
+
+def test_algorithmic_bytes_per_kernel(bench):
+    Np, Nc = 512 ** 3, 512 ** 3
+    assert bench.algorithmic_bytes("gather_kick_drift_deposit", Np, Nc, False) == 60 * Np + 4 * Nc
+    assert bench.algorithmic_bytes("gather_kick", Np, Nc, False) == 48 * Np + 4 * Nc
+    assert bench.algorithmic_bytes("deposit", Np, Nc, False) == 12 * Np + 4 * Nc
+    assert bench.algorithmic_bytes("gather_kick_drift_deposit", Np, Nc, True) == 2 * (60 * Np + 4 * Nc)
+    assert bench.algorithmic_bytes("fd_grad", Np, Nc, False) is None
+
+
+def test_dram_traffic_of_the_dominant_kernel_is_committed(bench):
+    w = bench.workload_name(9, 1)
+    t = bench.dram_traffic("gather_kick_drift_deposit", w)
+    assert t is not None and t > bench.algorithmic_bytes("gather_kick_drift_deposit", 512 ** 3, 512 ** 3, False)
+    assert bench.dram_traffic("no_such_kernel", w) is None
+
+
+def test_reference_arm_prints_one_json_line():
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"],
+                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["value"] > 0 and d["unit"] == "particle-steps/s" and d["higher_is_better"] is True
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
