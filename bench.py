@@ -78,20 +78,23 @@ class Clocks:
         self.samples = []  # (sm_mhz, max_mhz, set of reasons)
         self.thread = None
 
-    def _nvml_loop(self, nv, h):
-        import time as _t
+    def _nvml_sample(self):
+        nv, h = self.nv, self.h
         bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((float(sm), float(self.mx), {n for n, b in bits.items() if r & b}))
+        except Exception:
+            pass
+
+    def _nvml_loop(self):
+        import time as _t
         while not self.stop:
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append((float(sm), float(mx), {n for n, b in bits.items() if r & b}))
-            except Exception:
-                pass
+            self._nvml_sample()
             _t.sleep(0.01)
 
     def __enter__(self):
@@ -100,8 +103,9 @@ class Clocks:
             import threading
             import pynvml as nv
             nv.nvmlInit()
-            h = nv.nvmlDeviceGetHandleByIndex(self.index)
-            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.nv, self.h = nv, nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
             self.thread.start()
             return self
         except Exception:
@@ -116,8 +120,19 @@ class Clocks:
 
     def __exit__(self, *a):
         self.stop = True
+        self.smi_once = False
         if self.thread is not None:
             self.thread.join(timeout=2)
+            if not self.samples:  # a region shorter than the thread's start-up: one reading at its end
+                self._nvml_sample()
+            if not self.samples:  # NVML answered nothing: one nvidia-smi reading at the end
+                try:
+                    r = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                        "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=20)
+                    self._parse_smi(r.stdout)
+                    self.smi_once = True
+                except (OSError, subprocess.TimeoutExpired):
+                    pass
         if self.p:
             self.p.terminate()
             try:
@@ -125,23 +140,28 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.p.kill()
                 out, _ = self.p.communicate()
-            for l in out.splitlines():
-                f = [x.strip() for x in l.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    self.samples.append((float(f[1]), float(f[2]),
-                                         {n for n, v in zip(self.NAMES, f[5:9]) if v.lower().startswith("active")}))
-                except ValueError:
-                    continue
+            self._parse_smi(out)
+
+    def _parse_smi(self, out):
+        for l in out.splitlines():
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                self.samples.append((float(f[1]), float(f[2]),
+                                     {n for n, v in zip(self.NAMES, f[5:9]) if v.lower().startswith("active")}))
+            except ValueError:
+                continue
 
     def summary(self):
         sm = [x[0] for x in self.samples]
         mx = self.samples[-1][1] if self.samples else None
         reasons = set().union(*[x[2] for x in self.samples]) if self.samples else set()
+        source = "nvml 10 ms" if self.thread is not None else "nvidia-smi 200 ms"
+        if getattr(self, "smi_once", False):
+            source = "nvidia-smi once at the end (nvml gave no reading)"
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm),
-                "source": "nvml 10 ms" if self.thread is not None else "nvidia-smi 200 ms"}
+                "reasons": sorted(reasons), "samples": len(sm), "source": source}
 
 
 # ------------------------------------------------------------ distributed --

@@ -48,3 +48,60 @@ def test_reference_arm_prints_one_json_line():
     assert d["value"] > 0 and d["unit"] == "particle-steps/s" and d["higher_is_better"] is True
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+
+
+class _FakeNVML:
+    """Read-only NVML stand-in: a fixed SM clock and the power-cap reason."""
+    NVML_CLOCK_SM = 1
+    nvmlClocksEventReasonHwSlowdown = 1
+    nvmlClocksEventReasonHwThermalSlowdown = 2
+    nvmlClocksEventReasonSwThermalSlowdown = 4
+    nvmlClocksEventReasonSwPowerCap = 8
+
+    def nvmlInit(self):
+        pass
+
+    def nvmlDeviceGetHandleByIndex(self, i):
+        return i
+
+    def nvmlDeviceGetMaxClockInfo(self, h, kind):
+        return 1965
+
+    def nvmlDeviceGetClockInfo(self, h, kind):
+        return 1900
+
+    def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+        return 8
+
+
+@pytest.mark.parametrize("seconds", [0.0, 0.1])
+def test_clock_sampler_reports_short_and_long_regions(bench, monkeypatch, seconds):
+    """Clocks and throttle reasons are sampled during the timed region; a
+    region shorter than the sampling thread's start-up still gets a reading."""
+    import time
+    monkeypatch.setitem(sys.modules, "pynvml", _FakeNVML())
+    with bench.Clocks(0) as clk:
+        time.sleep(seconds)
+    s = clk.summary()
+    assert s["samples"] >= 1 and s["sm_mhz"] == 1900.0 and s["sm_max_mhz"] == 1965.0
+    assert s["reasons"] == ["sw_power_cap"] and s["source"] == "nvml 10 ms"
+
+
+class _SilentNVML(_FakeNVML):
+    def nvmlDeviceGetClockInfo(self, h, kind):
+        raise RuntimeError("no reading")
+
+
+def test_clock_sampler_survives_an_nvml_without_readings(bench, monkeypatch):
+    monkeypatch.setitem(sys.modules, "pynvml", _SilentNVML())
+    with bench.Clocks(0) as clk:
+        pass
+    s = clk.summary()
+    assert s["samples"] == 0 or s["source"].startswith("nvidia-smi")
+
+
+def test_nvidia_smi_lines_are_parsed(bench):
+    clk = bench.Clocks(0)
+    clk._parse_smi("0, 1900, 1965, 712.40, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n"
+                   "garbage line\n")
+    assert clk.samples == [(1900.0, 1965.0, {"sw_power_cap"})]
