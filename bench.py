@@ -164,6 +164,16 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm), "source": source}
 
 
+def clocks_disturbed(c):
+    """True for a clock record that rejects a timing: a hardware or thermal
+    slowdown, or a median SM clock below 90% of the maximum with no reason
+    active. The power cap alone (sw_power_cap) is normal and kept."""
+    if set(c.get("reasons", [])) & {"hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown"}:
+        return True
+    sm, mx = c.get("sm_mhz"), c.get("sm_max_mhz")
+    return bool(sm and mx and not c.get("reasons") and sm < 0.9 * mx)
+
+
 # ------------------------------------------------------------ distributed --
 def dist_init(n):
     if n <= 1:
@@ -443,9 +453,13 @@ def run_ours(args):
     # another job on the box): it is timed once more, and both are reported.
     # The decision is taken over all ranks so that every rank runs the same
     # collectives.
+    # The same holds for a run whose clock record shows a hardware or thermal
+    # slowdown, or SM clocks well below their maximum with no reason given
+    # (a clock lock left by someone else).
     prof_ms = sum(v[1] for v in prof.values())
     remeasured = None
-    if max_over_ranks(1.0 if prof_ms > 0 and ms32 > 1.15 * prof_ms else 0.0, dist) > 0:
+    slow = prof_ms > 0 and ms32 > 1.15 * prof_ms
+    if max_over_ranks(1.0 if slow or clocks_disturbed(clocks) else 0.0, dist) > 0:
         g2, ms_again, clocks_again, _ = timed_run("fp32")
         g2.close()
         remeasured = {"first_ms_per_step": ms32 / args.steps, "profile_ms_per_step": prof_ms / args.steps,

@@ -105,3 +105,12 @@ def test_nvidia_smi_lines_are_parsed(bench):
     clk._parse_smi("0, 1900, 1965, 712.40, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n"
                    "garbage line\n")
     assert clk.samples == [(1900.0, 1965.0, {"sw_power_cap"})]
+
+
+def test_clock_records_that_reject_a_timing(bench):
+    ok = {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": []}
+    assert not bench.clocks_disturbed(ok)
+    assert not bench.clocks_disturbed({"sm_mhz": 1300.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"]})
+    assert bench.clocks_disturbed({"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["hw_slowdown"]})
+    assert bench.clocks_disturbed({"sm_mhz": 1200.0, "sm_max_mhz": 1965.0, "reasons": []})
+    assert not bench.clocks_disturbed({"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0})
