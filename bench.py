@@ -210,7 +210,6 @@ def fof_bench(cb, Xh, n, dev, steps, reps=3):
     events, inputs resident in HBM), and end to end through conan_fof_run with
     host buffers. Size-independent checks: the same tags on every run, and the
     numbering of the groups in order of their lowest particle index."""
-    import numpy as np
     import torch
     Np = n ** 3
     ll = 0.2 * L_BOX / n
@@ -235,7 +234,6 @@ def fof_bench(cb, Xh, n, dev, steps, reps=3):
     big = int((mass >= 10).sum().item())
     largest = int(mass.max().item())
     del xd, td, first, cm, mass
-    tags_h = np.empty(Np, dtype=np.uint64)
     eng(Xh)  # warm-up of the host path
     t0 = time.perf_counter()
     tags_h, _ = eng(Xh)
