@@ -4,8 +4,11 @@
  * product: only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
  * load it, and the product never calls it. Every function restates the
  * reference algorithm it cites (paths relative to the reference project root)
- * in the same operation order, in double precision, single-threaded, so that
- * its results match the reference's own CPU run to rounding. It is pinned
+ * in the same operation order, in double precision, so that its results match
+ * the reference's own CPU run to rounding. Loops whose iterations each write
+ * only their own element (per particle or per cell) run on OpenMP threads, so
+ * the results do not depend on the thread count; every sum over particles or
+ * cells (the deposits, variances, dot products) runs serially in index order. It is pinned
  * against golden outputs written by the unmodified reference binary
  * (tests/golden/make_golden.py).
  *
@@ -229,6 +232,7 @@ void oracle_displacement(int R, int mbits, double L, const double *pot, double *
 void oracle_gradient(int R, int N, double L, const double *f, double *g) {
     size_t size = ipow(N, R);
     double res = L / N;
+#pragma omp parallel for schedule(static)
     for (size_t x = 0; x < size; ++x) {
         int p0[8], q[8];
         decode(x, R, N, p0);
@@ -255,6 +259,7 @@ void oracle_zeldovich(int R, int Nm, double L, const double *phi, double a_pos, 
     std::vector<double> u(size * R);
     oracle_gradient(R, Nm, L, phi, u.data());
     double cell = L / Nm; /* grid_space: x[i] * (L/N), src/base/box.hh:11-24 */
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i) {
         int q[8];
         decode(i, R, Nm, q);
@@ -375,6 +380,7 @@ void oracle_poisson(int R, int N, double L, double G, double a, double *delta) {
 void oracle_interp_gradient(int R, int N, double L, const double *phi, const double *X,
                             size_t n, double *out) {
     double res = L / N;
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; ++i) {
         double x[8], A[2][8], v[8] = {0};
         int origin[8];
@@ -434,6 +440,7 @@ void oracle_kick(int R, int Nm, int f, double L, double H0, double Om, double OL
     oracle_poisson(R, Nf, L, G, a, delta.data());
     double adot = oracle_adot(H0, Om, OL, a);
     oracle_interp_gradient(R, Nf, L, delta.data(), X, np, acc.data());
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < np; ++i)
         for (int k = 0; k < R; ++k) P[i * R + k] -= acc[i * R + k] * (da / adot);
     if (phi_out) std::memcpy(phi_out, delta.data(), nc * sizeof(double));
@@ -444,6 +451,7 @@ void oracle_drift(int R, int Nm, double H0, double Om, double OL, double *X, con
                   double a, double da) {
     size_t np = ipow(Nm, R);
     double adot = oracle_adot(H0, Om, OL, a);
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < np; ++i)
         for (int k = 0; k < R; ++k) X[i * R + k] += P[i * R + k] * (da / (a * a * adot));
 }
@@ -542,6 +550,7 @@ double dW(const double *A0, const double *A1, int R, int b, int k) {
 /* -sum_k FD4_k(U_k) / res on an R-cube (the adjoint of the FD4 gradient). */
 void neg_div(int R, int N, double res, const std::vector<std::vector<double>> &U, double *out) {
     size_t size = ipow(N, R);
+#pragma omp parallel for schedule(static)
     for (size_t x = 0; x < size; ++x) {
         int p0[8], q[8];
         decode(x, R, N, p0);
@@ -630,6 +639,7 @@ void oracle_diff_adjoint(int R, int mbits, int f, double L, double ns, int smoot
 
     /* ---- backward ---- */
     std::vector<double> Xb(np * R, 0.0), Pb(np * R, 0.0);
+#pragma omp parallel for schedule(static)
     for (size_t j = 0; j < np; ++j) {  // through the final deposit
         int o[8];
         double A0[8], A1[8];
@@ -664,6 +674,7 @@ void oracle_diff_adjoint(int R, int mbits, int f, double L, double ns, int smoot
         std::vector<double> div(nc), rhob(nc);
         neg_div(R, Nf, res_f, U, div.data());
         poisson_op(div.data(), rhob.data(), am);
+#pragma omp parallel for schedule(static)
         for (size_t j = 0; j < np; ++j) {
             double t1[8] = {0}, t2[8] = {0};
             int o[8];

@@ -131,6 +131,36 @@ double time_steps_t(int Nm, int f, double L, double H0, double Om, double OL, co
     return std::chrono::duration<double>(t2 - t1).count();
 }
 
+/* One solver state, one leapfrog step per entry of threads[]: step i runs
+ * with omp_set_num_threads(threads[i]) and its seconds go to seconds[i]. */
+template <unsigned R>
+double time_threads_t(int Nm, int f, double L, double H0, double Om, double OL, const double *phi,
+                      double a0, double da, int nt, const int *threads, double *seconds) {
+    auto mbox = BoxMaker(Nm, L).box<R>();
+    auto fbox = BoxMaker(f * Nm, L).box<R>();
+    Array<double> p(mbox->size());
+    for (size_t i = 0; i < mbox->size(); ++i) p[i] = phi[i];
+    Cosmology cosmos(H0, Om, OL);
+    QuietStdout quiet;
+    const int saved = omp_get_max_threads();
+    auto t0 = std::chrono::steady_clock::now();
+    Gravity<R> G("bench", mbox, fbox, p, cosmos, false, FMT_CONAN);
+    G.init(a0, a0 + da / 2);
+    auto t1 = std::chrono::steady_clock::now();
+    double a = a0;
+    for (int i = 0; i < nt; ++i) {
+        omp_set_num_threads(threads[i] > 0 ? threads[i] : saved);
+        auto s0 = std::chrono::steady_clock::now();
+        G.drift(a, da);
+        G.kick(a + da / 2, da);
+        auto s1 = std::chrono::steady_clock::now();
+        seconds[i] = std::chrono::duration<double>(s1 - s0).count();
+        a += da;
+    }
+    omp_set_num_threads(saved);
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
 }  // namespace
 
 extern "C" {
@@ -196,6 +226,19 @@ double ref_time_steps(int dim, int Nm, int f, double L, double H0, double Om, do
         case 1: return time_steps_t<1>(Nm, f, L, H0, Om, OL, phi, a0, da, n, t_init);
         case 2: return time_steps_t<2>(Nm, f, L, H0, Om, OL, phi, a0, da, n, t_init);
         case 3: return time_steps_t<3>(Nm, f, L, H0, Om, OL, phi, a0, da, n, t_init);
+    }
+    return -1;
+}
+
+/* Times one leapfrog step of the reference's Gravity<R> (src/run/nbody.hh:
+ * 97-133) per entry of threads[] (0: all threads) on one solver state, after
+ * one init; returns the init seconds, the steps' seconds in seconds[]. */
+double ref_time_threads(int dim, int Nm, int f, double L, double H0, double Om, double OL, const double *phi,
+                        double a0, double da, int nt, const int *threads, double *seconds) {
+    switch (dim) {
+        case 1: return time_threads_t<1>(Nm, f, L, H0, Om, OL, phi, a0, da, nt, threads, seconds);
+        case 2: return time_threads_t<2>(Nm, f, L, H0, Om, OL, phi, a0, da, nt, threads, seconds);
+        case 3: return time_threads_t<3>(Nm, f, L, H0, Om, OL, phi, a0, da, nt, threads, seconds);
     }
     return -1;
 }

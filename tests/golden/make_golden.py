@@ -134,7 +134,10 @@ def fof_goldens():
 
 def main():
     if not (REF / "conan_ref").exists():
-        subprocess.run(["make", "-C", str(ROOT / "oracle")], check=True)
+        src = os.environ.get("CONAN_REFERENCE_SRC")
+        if not src:
+            raise SystemExit("oracle/_ref/conan_ref is not built: set CONAN_REFERENCE_SRC to the reference's src/")
+        subprocess.run(["make", "-C", str(ROOT / "oracle"), f"REF={src}"], check=True)
     if sys.argv[1:] == ["fof"]:
         fof_goldens()
         print("fof fixtures written to", HERE)
