@@ -65,6 +65,7 @@ SIGNATURES = {
     "conan_last_error": (C.c_char_p, []),
     "conan_version": (C.c_char_p, []),
     "conan_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "conan_selftest_bounded_wait": (C.c_int, [C.c_uint, C.c_void_p]),
     "conan_ic_noise": (C.c_int, [C.POINTER(ICParams), _dp]),
     "conan_ic_generate": (C.c_int, [C.POINTER(ICParams), _dp, _dp]),
     "conan_ic_potential": (C.c_int, [C.POINTER(ICParams), _dp]),

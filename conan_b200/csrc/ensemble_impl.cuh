@@ -335,17 +335,7 @@ template <typename T, int R> struct Ens : EnsBase {
             v.p[k] += o;
         }
         v.np = np1;
-        CONAN_TRY(pm.ensure_xfer(np1 * R));
-        for (int which = 0; which < 2; ++which) {
-            double *dst = which == 0 ? X : Pm;
-            if (!dst) continue;
-            k_export<T, R><<<(unsigned)((np1 + 255) / 256), 256, 0, pm.st>>>(v, pm.res_f, which == 0 ? pm.xfer : nullptr,
-                                                                           which == 1 ? pm.xfer : nullptr);
-            CONAN_LAUNCHED();
-            CONAN_CUDA(cudaMemcpyAsync(dst, pm.xfer, np1 * R * sizeof(double), cudaMemcpyDeviceToHost, pm.st));
-            CONAN_CUDA(cudaStreamSynchronize(pm.st));
-        }
-        return CONAN_OK;
+        return pm.export_state(v, np1, X, Pm);
     }
 
     int last_ms(double *r, double *a) override {

@@ -20,9 +20,17 @@
 // Sharing rules: every call on a device uses the same array, so calls whose
 // GPU work overlaps in time (different streams, or different host threads
 // without ordering) race and give wrong densities; order them on one stream
-// or with events. The array keeps the last call's contents: each call clears
-// the cells it uses before depositing (and the conversion clears them again
-// after reading).
+// or with events. The array keeps the last call's contents, so each call
+// clears the cells it uses before depositing (one memset); the clear comes
+// first rather than last so that a call never depends on an earlier call
+// having run to the end.
+//
+// Window choice, as the conan_pm handle makes it: the largest lattice tile
+// whose shared-memory window fits and holds at most
+// LAG_WINDOW_CELLS_PER_PARTICLE window cells per particle; otherwise (fine
+// meshes, e.g. 32^3 particles on a 128^3 mesh) the largest tile with a
+// two-cell window, i.e. every corner goes to the accumulator with one
+// integer atomic. Both give the same integers.
 #include <mutex>
 
 #include "pm_kernels.cuh"
@@ -55,29 +63,47 @@ __global__ void __launch_bounds__(THREADS)
 }
 
 // Density contrast from the accumulator (units of 2^-23 particle weights,
-// times the particle mass), clearing the cells read.
-__global__ void __launch_bounds__(256) k_static_mesh(unsigned long long *__restrict__ acc, float *__restrict__ out,
-                                                     size_t n, double scale) {
+// times the particle mass).
+__global__ void __launch_bounds__(256) k_static_mesh(const unsigned long long *__restrict__ acc,
+                                                     float *__restrict__ out, size_t n, double scale) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const unsigned long long a = acc[i];
-    acc[i] = 0ull;
-    out[i] = (float)((double)a * (0x1p-23 * scale) - 1.0);
+    out[i] = (float)((double)acc[i] * (0x1p-23 * scale) - 1.0);
 }
 
-template <int R, int V> int window_of(int n, int f, LagWin *w, size_t *smem) {
+// Window of lattice tile V on an n^R lattice with f force cells per spacing:
+// 1 and the window when the tile fits the lattice and its window fits
+// shared memory, else 0. direct: a two-cell window (corners go to the
+// accumulator directly).
+template <int R, int V> int window_of(int n, int f, bool direct, LagWin *w, size_t *smem) {
     typedef LagTile<R, V> L;
     if (n < L::LX || (R >= 2 && n < L::LY) || (R == 3 && n < L::LZ)) return 0;
     LagWin x{};
-    x.w[0] = L::LX * f + L::M;
-    x.w[1] = R >= 2 ? L::LY * f + L::M : 1;
-    x.w[2] = R == 3 ? L::LZ * f + L::M : 1;
+    x.w[0] = direct ? 2 : L::LX * f + L::M;
+    x.w[1] = R >= 2 ? (direct ? 2 : L::LY * f + L::M) : 1;
+    x.w[2] = R == 3 ? (direct ? 2 : L::LZ * f + L::M) : 1;
     x.cells = (x.w[0] * x.w[1] * x.w[2] + 3) & ~3;
     size_t sh = (size_t)x.cells * LAG_PLANES * sizeof(uint32_t);
     if (sh > 112 * 1024) return 0;
     *w = x;
     *smem = sh;
     return 1;
+}
+
+template <int R, int V> constexpr double tile_particles() {
+    return (double)LagTile<R, V>::LX * LagTile<R, V>::LY * LagTile<R, V>::LZ;
+}
+
+// The tile variant and window for an n^R lattice on an (f n)^R mesh, as the
+// handle chooses them; -1 when the lattice is smaller than every tile.
+template <int R> int choose_window(int n, int f, LagWin *w, size_t *smem) {
+    int v = window_of<R, 0>(n, f, false, w, smem) ? 0 : window_of<R, 1>(n, f, false, w, smem) ? 1
+            : window_of<R, 2>(n, f, false, w, smem) ? 2 : -1;
+    const double per = v == 0 ? tile_particles<R, 0>() : v == 1 ? tile_particles<R, 1>() : tile_particles<R, 2>();
+    if (v < 0 || (double)w->cells > LAG_WINDOW_CELLS_PER_PARTICLE * per)
+        v = window_of<R, 0>(n, f, true, w, smem) ? 0 : window_of<R, 1>(n, f, true, w, smem) ? 1
+            : window_of<R, 2>(n, f, true, w, smem) ? 2 : -1;
+    return v;
 }
 
 template <int R, int V> int raise_smem_limit() {
@@ -132,13 +158,12 @@ template <int R>
 int deposit_static(int n, int f, const float *const *d, float *out, cudaStream_t st) {
     LagWin w{};
     size_t smem = 0;
-    int v = window_of<R, 0>(n, f, &w, &smem) ? 0 : window_of<R, 1>(n, f, &w, &smem) ? 1
-                                                 : window_of<R, 2>(n, f, &w, &smem) ? 2 : -1;
+    const int v = choose_window<R>(n, f, &w, &smem);
     if (v < 0)
         return set_error(CONAN_ERR_UNSUPPORTED,
-                         "conan_deposit_static: %d particles per side (f = %d) is below the smallest lattice tile "
+                         "conan_deposit_static: %d particles per side is below the smallest lattice tile (%d) "
                          "in %d dimensions",
-                         n, f, R);
+                         n, LagTile<R, 2>::LX, R);
     unsigned long long *acc = nullptr;
     CONAN_TRY(setup_device(&acc));
     const Mesh m = make_mesh(R, n * f, 1);

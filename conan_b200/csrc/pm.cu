@@ -30,6 +30,14 @@ int set_error(int code, const char *fmt, ...) {
     return code;
 }
 
+int err_word_status(int h) {
+    if (!h) return CONAN_OK;
+    if (h & 8)
+        return set_error(CONAN_ERR_TIMEOUT,
+                         "a bounded wait for a bulk tensor copy into shared memory ran out (code %d)", h);
+    return set_error(CONAN_ERR_STATE, "kernel self-check failed (code %d): corrupt cell offsets or payload", h);
+}
+
 double adot(double H0, double Om, double OL, double a) {
     // Cosmology::operator(), src/run/cosmology.hh:16-23.
     double Ok = 1 - Om - OL;
@@ -86,8 +94,12 @@ template <typename T, int R> struct PM : PMBase {
     uint32_t *count = nullptr, *off = nullptr, *rank = nullptr, *bsum = nullptr;
     int *err = nullptr;  // device error word set by kernel self-checks
     PE *pay = nullptr;
-    double *xfer = nullptr;
-    size_t xfer_n = 0;
+    // Host transfers pass through two staging chunks of stage_n doubles each,
+    // allocated at creation: no transfer allocates device memory, and the
+    // chunks alternate on the handle's stream.
+    double *stage[2] = {nullptr, nullptr};
+    size_t stage_n = 0;
+    static constexpr size_t STAGE_MAX = (size_t)1 << 24;  // doubles per chunk (128 MiB)
     void *work = nullptr;
     FFTPair fft;
     // FP32 3D FD4 meshes of 64..1024 cells per side: the Poisson solve as 2D
@@ -106,6 +118,7 @@ template <typename T, int R> struct PM : PMBase {
 
     ~PM() override {
         if (st) cudaStreamSynchronize(st);
+        if (gexec) cudaGraphExecDestroy(gexec);
         fft.destroy();
         fft2.destroy();
         for (void *p : allocs) cudaFree(p);
@@ -161,6 +174,9 @@ template <typename T, int R> struct PM : PMBase {
         size_t nb = (mf.cells + SCAN_CHUNK - 1) / SCAN_CHUNK;
         CONAN_TRY(alloc(&bsum, nb));
         CONAN_TRY(alloc(&pay, np * Pay<T>::words));
+        stage_n = std::min(STAGE_MAX, std::max(np * (size_t)R, std::max(mf.cells, mm.cells)));
+        CONAN_TRY(alloc(&stage[0], stage_n));
+        CONAN_TRY(alloc(&stage[1], stage_n));
         CONAN_TRY(alloc(&err, 1));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
         CONAN_CUDA(cudaMemsetAsync(count, 0, mf.cells * sizeof(uint32_t), st));
@@ -192,21 +208,40 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
-    int ensure_xfer(size_t n) {
-        if (xfer_n >= n) return CONAN_OK;
-        if (xfer) {
-            CONAN_CUDA(cudaStreamSynchronize(st));
-            for (auto it = allocs.begin(); it != allocs.end(); ++it)
-                if (*it == xfer) {
-                    allocs.erase(it);
-                    break;
-                }
-            cudaFree(xfer);
-            bytes -= xfer_n * sizeof(double);
-            xfer = nullptr;
+    // Particles per staging chunk (whole particles of R doubles).
+    size_t stage_particles() const { return stage_n / (size_t)R; }
+
+    // Absolute FP64 state of the n particles of view v into host X, Pm
+    // (either may be null), chunk by chunk through the staging buffers;
+    // returns after the last copy.
+    int export_state(const Parts<T> &v, size_t n, double *X, double *Pm) {
+        const size_t cp = stage_particles();
+        for (size_t i0 = 0; i0 < n; i0 += cp) {
+            const size_t cnt = std::min(cp, n - i0);
+            CONAN_TIMED(prof, "export", st,
+                        (k_export<T, R><<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(
+                            v, res_f, i0, cnt, X ? stage[0] : nullptr, Pm ? stage[1] : nullptr)));
+            if (X)
+                CONAN_CUDA(cudaMemcpyAsync(X + i0 * R, stage[0], cnt * R * sizeof(double), cudaMemcpyDeviceToHost,
+                                           st));
+            if (Pm)
+                CONAN_CUDA(cudaMemcpyAsync(Pm + i0 * R, stage[1], cnt * R * sizeof(double), cudaMemcpyDeviceToHost,
+                                           st));
         }
-        CONAN_TRY(alloc(&xfer, n));
-        xfer_n = n;
+        CONAN_CUDA(cudaStreamSynchronize(st));
+        return CONAN_OK;
+    }
+
+    // Converts n host doubles into the device array out (type T), chunk by
+    // chunk through the staging buffers.
+    int upload_mesh(const double *in, T *out, size_t n) {
+        for (size_t c0 = 0, b = 0; c0 < n; c0 += stage_n, b ^= 1) {
+            const size_t cnt = std::min(stage_n, n - c0);
+            CONAN_CUDA(cudaMemcpyAsync(stage[b], in + c0, cnt * sizeof(double), cudaMemcpyHostToDevice, st));
+            CONAN_TIMED(prof, "convert", st,
+                        (k_convert<double, T><<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(stage[b], out + c0, cnt,
+                                                                                          1.0, 0.0)));
+        }
         return CONAN_OK;
     }
 
@@ -308,7 +343,9 @@ template <typename T, int R> struct PM : PMBase {
                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
                     return CONAN_OK;
-            tma_smem = std::max(lag_smem, (size_t)(6 * L::LX * L::LY * L::LZ * 4 + 128));
+            const size_t stage_bytes = (size_t)(6 * L::LX * L::LY * L::LZ * 4 + 128);
+            // the window after the staged arrays, or over them
+            tma_smem = LAG_STAGE_KEEP ? stage_bytes + lag_smem : std::max(lag_smem, stage_bytes);
             auto kern = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
             if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem) != cudaSuccess) {
                 cudaGetLastError();
@@ -327,7 +364,7 @@ template <typename T, int R> struct PM : PMBase {
             if constexpr (R == 3 && V == 0) {
                 // staged drift+deposit: 1.87 against 2.33 ms at 512^3; with the
                 // gather the direct loads win (3.76 against 3.82 ms)
-                if (tma_ok && !c.kick) {
+                if (tma_ok && (LAG_TMA_GATHER || !c.kick)) {
                     auto tk = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
                     CONAN_TIMED(prof, name, st,
                                 (tk<<<(unsigned)tiles, L::THREADS, tma_smem, st>>>(P, mf, grad, c, lwin, lacc,
@@ -581,10 +618,7 @@ template <typename T, int R> struct PM : PMBase {
     // --- API ---------------------------------------------------------------
     int init(const double *phi, double apos, double amom) override {
         if (!phi) return set_error(CONAN_ERR_ARG, "null potential");
-        CONAN_TRY(ensure_xfer(mm.cells));
-        CONAN_CUDA(cudaMemcpyAsync(xfer, phi, mm.cells * sizeof(double), cudaMemcpyHostToDevice, st));
-        unsigned gb = (unsigned)((mm.cells + 255) / 256);
-        CONAN_TIMED(prof, "convert", st, (k_convert<double, T><<<gb, 256, 0, st>>>(xfer, mesh, mm.cells, 1.0, 0.0)));
+        CONAN_TRY(upload_mesh(phi, mesh, mm.cells));
         double cdz = -apos / (res_m * res_f), cpz = -amom / (res_m * res_f);
         CONAN_TIMED(prof, "zeldovich", st, (k_zeldovich<T, R><<<grid_p(), 256, 0, st>>>(P, mesh, mm, cdz, cpz)));
         CONAN_TRY(positions_reset());
@@ -628,6 +662,47 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
+    // The instantiated graph of the last run segment. A later segment of the
+    // same shape (the same launches with other scale-factor coefficients)
+    // updates it in place instead of instantiating a new one.
+    cudaGraphExec_t gexec = nullptr;
+
+    // Steps [i0, i1) captured into a CUDA graph and launched; returns after
+    // the graph has run.
+    int graph_segment(double &a, double da, unsigned i0, unsigned i1) {
+        cudaGraph_t g = nullptr;
+        CONAN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int rc = steps(a, da, i0, i1);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (rc != CONAN_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return set_error(CONAN_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        bool updated = false;
+        if (gexec) {
+            cudaGraphExecUpdateResultInfo info{};
+            if (cudaGraphExecUpdate(gexec, g, &info) == cudaSuccess) {
+                updated = true;
+            } else {  // another shape: instantiate anew
+                cudaGetLastError();
+                cudaGraphExecDestroy(gexec);
+                gexec = nullptr;
+            }
+        }
+        cudaError_t ie = updated ? cudaSuccess : cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            gexec = nullptr;
+            return set_error(CONAN_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
+        }
+        cudaError_t le = cudaGraphLaunch(gexec, st);
+        cudaError_t se = cudaStreamSynchronize(st);
+        if (le != cudaSuccess) return set_error(CONAN_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(le));
+        if (se != cudaSuccess) return set_error(CONAN_ERR_CUDA, "graph execution failed: %s", cudaGetErrorString(se));
+        return CONAN_OK;
+    }
+
     int run(conan_pm *h, const double *phi, double a0, double da, unsigned n, conan_step_cb cb,
             void *user) override {
         if (phi) CONAN_TRY(init(phi, a0, a0 + da / 2));
@@ -641,28 +716,7 @@ template <typename T, int R> struct PM : PMBase {
                 if (seg_end > n) seg_end = n;
             }
             if (!prof.on && !debug_sync()) {
-                cudaGraph_t g = nullptr;
-                CONAN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                int rc = steps(a, da, i, seg_end);
-                cudaError_t ce = cudaStreamEndCapture(st, &g);
-                if (rc != CONAN_OK) {
-                    if (g) cudaGraphDestroy(g);
-                    return rc;
-                }
-                if (ce != cudaSuccess)
-                    return set_error(CONAN_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
-                cudaGraphExec_t ex = nullptr;
-                cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
-                cudaGraphDestroy(g);
-                if (ie != cudaSuccess)
-                    return set_error(CONAN_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
-                cudaError_t le = cudaGraphLaunch(ex, st);
-                cudaError_t se = cudaStreamSynchronize(st);
-                cudaGraphExecDestroy(ex);
-                if (le != cudaSuccess)
-                    return set_error(CONAN_ERR_CUDA, "graph launch failed: %s", cudaGetErrorString(le));
-                if (se != cudaSuccess)
-                    return set_error(CONAN_ERR_CUDA, "graph execution failed: %s", cudaGetErrorString(se));
+                CONAN_TRY(graph_segment(a, da, i, seg_end));
             } else {
                 CONAN_TRY(steps(a, da, i, seg_end));
             }
@@ -683,31 +737,25 @@ template <typename T, int R> struct PM : PMBase {
         CONAN_CUDA(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         CONAN_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
         CONAN_CUDA(cudaStreamSynchronize(st));
-        if (h) return set_error(CONAN_ERR_STATE, "kernel self-check failed (code %d): corrupt cell offsets", h);
-        return CONAN_OK;
+        return err_word_status(h);
     }
 
     int get_state(double *X, double *Pm) override {
-        CONAN_TRY(ensure_xfer(np * R));
-        for (int which = 0; which < 2; ++which) {
-            double *dst = which == 0 ? X : Pm;
-            if (!dst) continue;
-            CONAN_TIMED(prof, "export", st,
-                        (k_export<T, R><<<grid_p(), 256, 0, st>>>(P, res_f, which == 0 ? xfer : nullptr,
-                                                                  which == 1 ? xfer : nullptr)));
-            CONAN_CUDA(cudaMemcpyAsync(dst, xfer, np * R * sizeof(double), cudaMemcpyDeviceToHost, st));
-            CONAN_CUDA(cudaStreamSynchronize(st));
-        }
+        CONAN_TRY(export_state(P, np, X, Pm));
         return check_err();
     }
 
     int set_state(const double *X, const double *Pm, double apos, double amom) override {
         if (!X || !Pm) return set_error(CONAN_ERR_ARG, "null state");
-        size_t n = np * R;
-        CONAN_TRY(ensure_xfer(2 * n));
-        CONAN_CUDA(cudaMemcpyAsync(xfer, X, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        CONAN_CUDA(cudaMemcpyAsync(xfer + n, Pm, n * sizeof(double), cudaMemcpyHostToDevice, st));
-        CONAN_TIMED(prof, "import", st, (k_import<T, R><<<grid_p(), 256, 0, st>>>(P, res_f, xfer, xfer + n)));
+        const size_t cp = stage_particles();
+        for (size_t i0 = 0; i0 < np; i0 += cp) {
+            const size_t cnt = std::min(cp, np - i0);
+            CONAN_CUDA(cudaMemcpyAsync(stage[0], X + i0 * R, cnt * R * sizeof(double), cudaMemcpyHostToDevice, st));
+            CONAN_CUDA(cudaMemcpyAsync(stage[1], Pm + i0 * R, cnt * R * sizeof(double), cudaMemcpyHostToDevice, st));
+            CONAN_TIMED(prof, "import", st,
+                        (k_import<T, R><<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(P, res_f, i0, cnt, stage[0],
+                                                                                       stage[1])));
+        }
         CONAN_TRY(positions_reset());
         a_pos = apos;
         a_mom = amom;
@@ -716,10 +764,13 @@ template <typename T, int R> struct PM : PMBase {
     }
 
     int mesh_out(double *out) {
-        CONAN_TRY(ensure_xfer(mf.cells));
-        unsigned gb = (unsigned)((mf.cells + 255) / 256);
-        CONAN_TIMED(prof, "convert", st, (k_convert<T, double><<<gb, 256, 0, st>>>(mesh, xfer, mf.cells, 1.0, 0.0)));
-        CONAN_CUDA(cudaMemcpyAsync(out, xfer, mf.cells * sizeof(double), cudaMemcpyDeviceToHost, st));
+        for (size_t c0 = 0, b = 0; c0 < mf.cells; c0 += stage_n, b ^= 1) {
+            const size_t cnt = std::min(stage_n, mf.cells - c0);
+            CONAN_TIMED(prof, "convert", st,
+                        (k_convert<T, double><<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(mesh + c0, stage[b], cnt,
+                                                                                          1.0, 0.0)));
+            CONAN_CUDA(cudaMemcpyAsync(out + c0, stage[b], cnt * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
         CONAN_CUDA(cudaStreamSynchronize(st));
         return check_err();
     }
@@ -866,6 +917,22 @@ PMBase *make_pm(const conan_pm_params &p) {
 
 using namespace conan;
 
+namespace conan {
+
+// One CTA waits on a shared-memory barrier that nothing completes, with the
+// bounded wait of the staged kernels; the wait must run out (bit 3).
+__global__ void k_wait_selftest(int *err, unsigned polls) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !tma_wait(&bar, polls)) atomicOr(err, 8);
+}
+
+}  // namespace conan
+
 struct conan_pm {
     PMBase *impl;
 };
@@ -890,6 +957,25 @@ int conan_device_count(int *n) {
     }
     *n = c;
     return CONAN_OK;
+}
+
+int conan_selftest_bounded_wait(unsigned polls, void *stream) {
+    int dev = 0;
+    CONAN_CUDA(cudaGetDevice(&dev));
+    CONAN_TRY(device_guard(dev));
+    cudaStream_t st = (cudaStream_t)stream;
+    int *err = nullptr, h = 0;
+    CONAN_CUDA(cudaMalloc(&err, sizeof(int)));
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+        k_wait_selftest<<<1, 32, 0, st>>>(err, polls);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(err);
+    if (e != cudaSuccess) return set_error(CONAN_ERR_CUDA, "bounded-wait self-test: %s", cudaGetErrorString(e));
+    return err_word_status(h);
 }
 
 conan_pm *conan_pm_create(const conan_pm_params *p) {

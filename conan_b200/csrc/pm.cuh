@@ -12,6 +12,10 @@ namespace conan {
 // Scale-factor rate adot(a) (Cosmology::operator(), src/run/cosmology.hh:16-23).
 double adot(double H0, double Om, double OL, double a);
 int check_pm_params(const conan_pm_params *p);
+// Status of a kernel error word (CONAN_OK when 0): bit 3 (value 8), a
+// bounded wait for a bulk copy that ran out, is CONAN_ERR_TIMEOUT; the
+// other bits are failed self-checks of the deposit (CONAN_ERR_STATE).
+int err_word_status(int h);
 // Selects device `dev`, failing with a message when there is none.
 int device_guard(int dev);
 

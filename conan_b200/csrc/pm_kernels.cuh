@@ -781,21 +781,96 @@ template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1
 // STAGED: the tile's d[0..2], p[0..2] arrive in shared memory (six
 // LX*LY*LZ arrays in tile order, see k_gkd_lag_tma), particle group j
 // signalled by bars[j]; otherwise they are read from global memory.
-__device__ inline void tma_wait(unsigned long long *bar, int *err);
+__device__ inline bool tma_wait(unsigned long long *bar, unsigned limit);
+constexpr unsigned TMA_WAIT_LIMIT = 1u << 20;  // polls of try_wait (about a second at most)
+
+// Deposit position of a displacement d (force cells) along one axis: d
+// rounded to 2^-21 cell, Q = rn(d 2^21), cell offset Q >> 21 (floor) and
+// fraction Q & (2^21 - 1), as Pay<float>::cell_frac. 32-bit integer
+// arithmetic while |d 2^21| < 2^31 (displacements below 1024 cells), 64-bit
+// beyond; both give the same integers.
+__device__ __forceinline__ void quant_pos(float d, int *cell, uint32_t *fr) {
+    const float s = d * 2097152.0f;
+    if (fabsf(s) < 2147483648.0f) {
+        const int Q = __float2int_rn(s);
+        *cell = Q >> 21;
+        *fr = (uint32_t)Q & 0x1FFFFFu;
+    } else {
+        const long long Q = __float2ll_rn(s);
+        *cell = (int)(Q >> 21);
+        *fr = (uint32_t)(Q & 0x1FFFFF);
+    }
+}
+
+// CIC force of one particle from the packed FD4 gradient mesh Gm of its
+// member (gather_force<float, R, false> with 32-bit corner offsets; same
+// operations in the same order): q lattice point in force cells, d its
+// displacement.
+template <int R>
+__device__ __forceinline__ void gather_g4(const G4<float> *__restrict__ Gm, int shift, uint32_t mask, const int *q,
+                                          const float *d, bool periodic, float *F) {
+    int o[3] = {0, 0, 0};
+    float a1[3] = {0.f, 0.f, 0.f}, a0[3] = {1.f, 1.f, 1.f};
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        gather_axis<float>(d[k], q[k], periodic, &o[k], &a1[k]);
+        a0[k] = 1.0f - a1[k];
+    }
+    uint32_t off[3][2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        off[k][0] = k < R ? ((uint32_t)o[k] & mask) << (k * shift) : 0u;
+        off[k][1] = k < R ? ((uint32_t)(o[k] + 1) & mask) << (k * shift) : 0u;
+    }
+    // z = ((1 a_x) a_y) a_z, as the loop of gather_force multiplies
+    float wxy[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) wxy[b] = (b & 1 ? a1[0] : a0[0]) * (R >= 2 ? (b & 2 ? a1[1] : a0[1]) : 1.0f);
+    F[0] = F[1] = F[2] = 0.0f;
+#pragma unroll
+    for (int b = 0; b < (1 << R); ++b) {
+        const uint32_t ci = off[0][b & 1] + off[1][(b >> 1) & 1] + off[2][(b >> 2) & 1];
+        const float z = R == 3 ? wxy[b & 3] * ((b & 4) ? a1[2] : a0[2]) : wxy[b & 3];
+        const G4<float> gv = load_g4(Gm + ci);
+        F[0] += gv.x * z;
+        if (R > 1) F[1] += gv.y * z;
+        if (R > 2) F[2] += gv.z * z;
+    }
+}
+
+// Staged tiles keep the drifted displacements in the staging memory and
+// place the window after it (instead of over it): the deposit reads the
+// particles back from shared memory, not from registers. A compile-time
+// tunable.
+#ifndef LAG_STAGE_KEEP
+#define LAG_STAGE_KEEP 0
+#endif
+// The gather + kick + drift + deposit launches staged too (not only the
+// first drift + deposit); a compile-time tunable.
+#ifndef LAG_TMA_GATHER
+#define LAG_TMA_GATHER 0
+#endif
 
 template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED, bool STAGED = false>
 __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
                                          unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
-                                         const GKD &gc, const float *stage = nullptr,
-                                         unsigned long long *bars = nullptr, int *err = nullptr) {
+                                         const GKD &gc, float *stage = nullptr,
+                                         unsigned long long *bars = nullptr, int *err = nullptr,
+                                         int *stage_fail = nullptr) {
     constexpr int NT = LX * LY * LZ;
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
     constexpr int NW = THREADS / 32;
-    extern __shared__ __align__(16) uint32_t lag_sh[];
+    constexpr bool KEEP = STAGED && LAG_STAGE_KEEP;
+    extern __shared__ __align__(16) uint32_t lag_dyn[];
+    uint32_t *lag_sh = KEEP ? reinterpret_cast<uint32_t *>(stage + 6 * NT) : lag_dyn;  // the window
     __shared__ int wred[6][NW];
     __shared__ int org[6];  // window origin per axis, then the extent of the box to flush
     const int cells = win.cells;
+    if constexpr (KEEP) {  // the window is free from the start: clear it while the copies arrive
+        uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
+        for (int c = threadIdx.x; c < cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    }
 
     const int s = P.mshift;
     const int ntx = (1 << s) / LX, nty = R >= 2 ? (1 << s) / LY : 1, ntz = R == 3 ? (1 << s) / LZ : 1;
@@ -807,57 +882,76 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     const size_t pbase = (size_t)member << P.bshift;
     const size_t cb = (size_t)member << m.cshift;
     const int f = P.f;
+    const uint32_t mask = (uint32_t)m.n - 1;
+    // this member's arrays: every index below is a 32-bit offset into them
+    float *dm[3];
+    float *pm[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        dm[k] = k < R ? P.d[k] + pbase : nullptr;
+        pm[k] = k < R ? P.p[k] + pbase : nullptr;
+    }
+    unsigned long long *__restrict__ accm = acc + cb;
 
     // displacements of this thread's particles (their cells and fractions
     // are recomputed from these when depositing) and the box of their cells
-    float dd[NPT][3];
+    float dd[KEEP ? 1 : NPT][3];
     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
         const int t = (int)threadIdx.x + j * THREADS;
         const int lx = t % LX, ly = (t / LX) % LY, lz = t / (LX * LY);
         const int c[3] = {tx0 + lx, ty0 + ly, tz0 + lz};
-        size_t i = pbase + (size_t)c[0];
-        if (R >= 2) i += (size_t)c[1] << s;
-        if (R == 3) i += (size_t)c[2] << (2 * s);
+        uint32_t i = (uint32_t)c[0];
+        if (R >= 2) i += (uint32_t)c[1] << s;
+        if (R == 3) i += (uint32_t)c[2] << (2 * s);
         float d[3];
         if constexpr (FUSED) {
             float p[3];
 #pragma unroll
             for (int k = 0; k < R; ++k) {  // read once: evict-first, L1 stays for the gradients
                 if constexpr (STAGED) {
-                    if (k == 0) tma_wait(bars + j, err);  // group j: this thread's particle j
+                    // group j holds this thread's particle j
+                    if (k == 0 && !tma_wait(bars + j, TMA_WAIT_LIMIT)) {
+                        atomicOr(err, 8);
+                        *stage_fail = 1;
+                    }
                     d[k] = stage[k * NT + t];
                     p[k] = stage[(3 + k) * NT + t];
                 } else {
-                    d[k] = __ldcs(P.d[k] + i);
-                    p[k] = __ldcs(P.p[k] + i);
+                    d[k] = __ldcs(dm[k] + i);
+                    p[k] = __ldcs(pm[k] + i);
                 }
             }
             if (gc.kick) {
                 float F[3];
-                gather_force<float, R, false>(P, m, i, nullptr, nullptr, G, gc.periodic, d, F);
+                const int q[3] = {c[0] * f, R >= 2 ? c[1] * f : 0, R == 3 ? c[2] * f : 0};
+                gather_g4<R>(G + cb, m.shift, mask, q, d, gc.periodic, F);
                 const float ck = (float)gc.ck;
 #pragma unroll
                 for (int k = 0; k < R; ++k) {
                     p[k] -= F[k] * ck;
-                    P.p[k][i] = p[k];
+                    __stcs(pm[k] + i, p[k]);
                 }
             }
             const float cd = (float)gc.cd;
 #pragma unroll
             for (int k = 0; k < R; ++k) {
                 d[k] += p[k] * cd;
-                P.d[k][i] = d[k];
+                __stcs(dm[k] + i, d[k]);
+                if constexpr (KEEP) stage[k * NT + t] = d[k];
             }
         } else {
 #pragma unroll
-            for (int k = 0; k < R; ++k) d[k] = __ldg(P.d[k] + i);
+            for (int k = 0; k < R; ++k) d[k] = __ldg(dm[k] + i);
         }
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            dd[j][k] = d[k];
-            const int uk = c[k] * f + (int)(__float2ll_rn(d[k] * 2097152.0f) >> 21);
+            if constexpr (!KEEP) dd[j][k] = d[k];
+            int ck;
+            uint32_t fk;
+            quant_pos(d[k], &ck, &fk);
+            const int uk = c[k] * f + ck;
             lo[k] = min(lo[k], uk);
             hi[k] = max(hi[k], uk);
         }
@@ -871,9 +965,21 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             wred[3 + k][wid] = b;
         }
     }
-    if constexpr (STAGED) __syncthreads();  // staged particles are read before the window reuses the memory
-    uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
-    for (int c = threadIdx.x; c < cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    if constexpr (STAGED) {
+        __syncthreads();  // staged particles are read before the window reuses the memory
+        if (*stage_fail) {
+            // a copy did not arrive in time: wait (bounded again) for the
+            // copies still in flight into this memory, then deposit nothing
+            if (threadIdx.x == 0)
+                for (int j = 0; j < NPT; ++j) tma_wait(bars + j, TMA_WAIT_LIMIT);
+            __syncthreads();
+            return;
+        }
+    }
+    if constexpr (!KEEP) {
+        uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
+        for (int c = threadIdx.x; c < cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    }
     __syncthreads();
     if (threadIdx.x < R) {
         const int k = threadIdx.x;
@@ -892,8 +998,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     __syncthreads();
 
     const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
-    const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2];
-    const int mask = m.n - 1;
+    const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2], W01 = W0 * W1;
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
         // cells (unwrapped) and 21-bit fractions of the deposit position
@@ -904,9 +1009,9 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             const int c[3] = {tx0 + t % LX, ty0 + (t / LX) % LY, tz0 + t / (LX * LY)};
 #pragma unroll
             for (int k = 0; k < R; ++k) {
-                long long Q = __float2ll_rn(dd[j][k] * 2097152.0f);
-                u[k] = c[k] * f + (int)(Q >> 21);
-                fr[k] = (uint32_t)(Q & 0x1FFFFF);
+                int ck;
+                quant_pos(KEEP ? stage[k * NT + t] : dd[j][k], &ck, &fr[k]);
+                u[k] = c[k] * f + ck;
             }
         }
         float f0 = (float)fr[0] * 0x1p-21f;
@@ -929,7 +1034,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                const int wc = base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W0 * W1;
+                const int wc = base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W01;
                 if constexpr (LAG_PLANES == 2) {
                     Slot<float>::add(lag_sh, wc, v, cells);
                 } else if (v) {
@@ -937,10 +1042,10 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
                     // accumulator mesh directly (rare: over 2^9 particles' weight)
                     const uint32_t old = atomicAdd(lag_sh + wc, v);
                     if (old + v < old) {
-                        size_t g = (size_t)((u[0] + (b & 1)) & mask);
-                        if (R >= 2) g |= (size_t)((u[1] + ((b >> 1) & 1)) & mask) << m.shift;
-                        if (R == 3) g |= (size_t)((u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
-                        atomicAdd(acc + cb + g, 1ull << 32);
+                        uint32_t g = (uint32_t)(u[0] + (b & 1)) & mask;
+                        if (R >= 2) g |= ((uint32_t)(u[1] + ((b >> 1) & 1)) & mask) << m.shift;
+                        if (R == 3) g |= ((uint32_t)(u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+                        atomicAdd(accm + g, 1ull << 32);
                     }
                 }
             }
@@ -948,10 +1053,10 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
 #pragma unroll
             for (int b = 0; b < (1 << R); ++b) {
                 uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                size_t g = (size_t)((u[0] + (b & 1)) & mask);
-                if (R >= 2) g |= (size_t)((u[1] + ((b >> 1) & 1)) & mask) << m.shift;
-                if (R == 3) g |= (size_t)((u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
-                if (v) atomicAdd(acc + cb + g, (unsigned long long)v);
+                uint32_t g = (uint32_t)(u[0] + (b & 1)) & mask;
+                if (R >= 2) g |= ((uint32_t)(u[1] + ((b >> 1) & 1)) & mask) << m.shift;
+                if (R == 3) g |= ((uint32_t)(u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+                if (v) atomicAdd(accm + g, (unsigned long long)v);
             }
         }
     }
@@ -968,10 +1073,10 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
         const int wc = (l2 * W1 + l1) * W0 + l0;
         uint32_t a = lag_sh[wc], b = LAG_PLANES == 2 ? lag_sh[cells + wc] : 0u;
         if (a | b) {
-            size_t g = (size_t)((o0 + l0) & mask);
-            if (R >= 2) g |= (size_t)((o1 + l1) & mask) << m.shift;
-            if (R == 3) g |= (size_t)((o2 + l2) & mask) << (2 * m.shift);
-            atomicAdd(acc + cb + g, ((unsigned long long)b << 32) | a);
+            uint32_t g = (uint32_t)(o0 + l0) & mask;
+            if (R >= 2) g |= ((uint32_t)(o1 + l1) & mask) << m.shift;
+            if (R == 3) g |= ((uint32_t)(o2 + l2) & mask) << (2 * m.shift);
+            atomicAdd(accm + g, ((unsigned long long)b << 32) | a);
         }
         l0 += s0;
         l1 += s1;
@@ -1010,27 +1115,29 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 // Thread 0 issues the bulk tensor copies of all groups at once, each group
 // completing its own mbarrier, and every thread waits for group j just
 // before it needs particle j, so the first particles are computed while the
-// rest arrive. Waits are bounded: after TMA_WAIT_LIMIT polls a wait sets bit
-// 8 of the error word and goes on. No multicast: every copy reads this GPU's
-// own memory into this CTA.
+// rest arrive. Waits are bounded: a wait that runs out after TMA_WAIT_LIMIT
+// polls sets bit 3 (value 8) of the error word (CONAN_ERR_TIMEOUT on the
+// host) and the tile, after one more bounded wait for its copies in flight,
+// deposits nothing. No multicast: every copy reads this GPU's own memory into
+// this CTA.
 struct TileMaps {
     CUtensorMap a[6];  // d0, d1, d2, p0, p1, p2; box LX x LY x (LZ / NPT)
 };
 
-constexpr unsigned TMA_WAIT_LIMIT = 1u << 20;  // polls of try_wait (about a second at most)
-
 __device__ inline uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ inline void tma_wait(unsigned long long *bar, int *err) {
+// Waits for phase 0 of mbarrier `bar`, at most `limit` polls; false when
+// the wait ran out.
+__device__ inline bool tma_wait(unsigned long long *bar, unsigned limit) {
     const uint32_t b = smem_addr(bar);
     uint32_t done = 0;
-    for (unsigned it = 0; it < TMA_WAIT_LIMIT && !done; ++it)
+    for (unsigned it = 0; it < limit && !done; ++it)
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
             : "=r"(done)
             : "r"(b)
             : "memory");
-    if (!done) atomicOr(err, 8);
+    return done != 0;
 }
 
 template <int R, int LX, int LY, int LZ, int THREADS>
@@ -1042,6 +1149,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     static_assert(GZ * NPT == LZ && GZ * LX * LY == THREADS, "a group of z-planes holds one particle per thread");
     extern __shared__ __align__(16) uint32_t lag_sh[];
     __shared__ __align__(8) unsigned long long bars[NPT];
+    __shared__ int stage_fail;
     // bulk tensor copies land on 128-byte boundaries (the launch adds 128 bytes)
     float *stage = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(lag_sh) + 127) & ~(uintptr_t)127);
     const int s = P.mshift;
@@ -1051,6 +1159,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     const int x0 = (int)(tile % ntx) * LX, y0 = (int)((tile / ntx) % nty) * LY;
     const int z0 = (int)(tile / (ntx * nty)) * LZ + (int)(member << s);
     if (threadIdx.x == 0) {
+        stage_fail = 0;
 #pragma unroll
         for (int j = 0; j < NPT; ++j) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bars + j)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1071,7 +1180,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
                     : "memory");
         }
     }
-    lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage, bars, err);
+    lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage, bars, err, &stage_fail);
 }
 
 // Density contrast from the integer accumulator (units of 2^-23 particle
@@ -1121,31 +1230,36 @@ __global__ void k_zeldovich(Parts<T> P, const T *__restrict__ phim, Mesh mm, dou
     }
 }
 
-// Absolute positions / momenta (AoS doubles) from the lattice state.
+// Absolute positions / momenta (AoS doubles) of particles i0 .. i0+cnt-1
+// from the lattice state, written from X[0], Pm[0] on (either may be null).
 template <typename T, int R>
-__global__ void k_export(Parts<T> P, double res, double *__restrict__ X, double *__restrict__ Pm) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.np) return;
+__global__ void k_export(Parts<T> P, double res, size_t i0, size_t cnt, double *__restrict__ X,
+                         double *__restrict__ Pm) {
+    const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= cnt) return;
+    const size_t i = i0 + j;
     int q[3];
     lattice<T, R>(P, i, q);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        if (X) X[i * R + k] = ((double)q[k] + (double)P.d[k][i]) * res;
-        if (Pm) Pm[i * R + k] = (double)P.p[k][i] * res;
+        if (X) X[j * R + k] = ((double)q[k] + (double)P.d[k][i]) * res;
+        if (Pm) Pm[j * R + k] = (double)P.p[k][i] * res;
     }
 }
 
+// The inverse of k_export for particles i0 .. i0+cnt-1.
 template <typename T, int R>
-__global__ void k_import(Parts<T> P, double res, const double *__restrict__ X,
+__global__ void k_import(Parts<T> P, double res, size_t i0, size_t cnt, const double *__restrict__ X,
                          const double *__restrict__ Pm) {
-    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.np) return;
+    const size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= cnt) return;
+    const size_t i = i0 + j;
     int q[3];
     lattice<T, R>(P, i, q);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        P.d[k][i] = (T)(X[i * R + k] / res - (double)q[k]);
-        P.p[k][i] = (T)(Pm[i * R + k] / res);
+        P.d[k][i] = (T)(X[j * R + k] / res - (double)q[k]);
+        P.p[k][i] = (T)(Pm[j * R + k] / res);
     }
 }
 

@@ -53,6 +53,15 @@ const char *conan_last_error(void);
 const char *conan_version(void);
 /* Number of visible CUDA devices (0 without a GPU). */
 int conan_device_count(int *n);
+/* Health check of the failure path of the kernels' bounded waits (no
+ * reference counterpart: the reference has no GPU waits). One CTA on the
+ * current device waits, `polls` polls at most, on a shared-memory barrier
+ * that nothing completes, with the wait the TMA-staged kernels use; the wait
+ * runs out, and the call returns CONAN_ERR_TIMEOUT as those kernels' host
+ * check does. Any other result is a fault in that path. The context stays
+ * usable. stream: cudaStream_t (NULL: default stream); returns after the
+ * kernel. */
+int conan_selftest_bounded_wait(unsigned polls, void *stream);
 
 /* ------------------------------------------------------------------ ic -- */
 

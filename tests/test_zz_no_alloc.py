@@ -35,8 +35,11 @@ def _static(lib, dim, n, f, d, stream):
     return rc, dt, out
 
 
+# fine meshes (3D f = 4 and 8, 2D f = 8: 128^3 and 1024^2 cells) take the
+# two-cell window, where every corner goes to the accumulator directly
 @pytest.mark.parametrize("dim,n,f,amp", [(3, 32, 1, 3.0), (3, 64, 2, 12.0), (3, 8, 2, 40.0), (2, 256, 1, 30.0),
-                                         (2, 32, 4, 5.0), (1, 1024, 2, 300.0)])
+                                         (2, 32, 4, 5.0), (1, 1024, 2, 300.0), (3, 32, 4, 6.0), (3, 16, 8, 20.0),
+                                         (2, 128, 8, 10.0)])
 def test_static_deposit_matches_pm_density(gpu, conan, dim, n, f, amp):
     from conan_b200 import _lib as L
     lib = L.lib()
