@@ -291,72 +291,136 @@ def fof_tool_vs_reference(cb, n_sample=128, max_seconds=60.0):
 
 
 # ------------------------------------------------------------- reference --
-def cpu_reference(mbits_sample=7, max_seconds=20.0, threads=None, max_steps=None):
-    """Times the reference's own Gravity<3>::drift+kick (oracle/_ref, compiled
-    from the reference sources; falls back to the CPU restatement) on a
-    bounded sample: a 128^3-particle / 128^3-mesh box with the throughput
-    box's cell size (L scaled to 125 Mpc/h), same spectrum and time step."""
+def _reference_lib():
+    """The reference's own code compiled from its sources (oracle/_ref), or None."""
     import ctypes
-    import numpy as np
-    from oracle import cpu as oracle
-    n = 1 << mbits_sample
-    L = L_BOX * n / 512
-    noise = oracle.noise_mt19937(3, n ** 3)
-    phi = oracle.potential(3, mbits_sample, L, oracle.grf_scale_free(3, mbits_sample, L, NS, False, 8.0, 0.83, noise))
     reflib = ROOT / "oracle" / "_ref" / "libconan_ref.so"
-    cores = threads or os.cpu_count()
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    steps = 0
-    total = 0.0
-    if reflib.exists():
-        R = ctypes.CDLL(str(reflib))
-        R.ref_time_steps.restype = ctypes.c_double
-        R.ref_max_threads.restype = ctypes.c_int
-        cores = R.ref_max_threads()
+    if not reflib.exists():
+        return None
+    R = ctypes.CDLL(str(reflib))
+    R.ref_time_threads.restype = ctypes.c_double
+    R.ref_max_threads.restype = ctypes.c_int
+    return R
+
+
+def _reference_potential(mbits, L, seed=3):
+    """The box's potential on the CPU from the reference's mt19937 white noise
+    (CPU restatement of _generate_random_field and _compute_potential,
+    src/ic/ic.cc:37-117); not timed."""
+    from oracle import cpu as oracle
+    noise = oracle.noise_mt19937(seed, (1 << mbits) ** 3)
+    return oracle.potential(3, mbits, L, oracle.grf_scale_free(3, mbits, L, NS, False, 8.0, 0.83, noise))
+
+
+def cpu_reference(mbits=9, threads=(0, 1)):
+    """Times the reference's own PM step, Gravity<3>::drift + kick
+    (src/run/nbody.hh:97-133, compiled from its sources into oracle/_ref), on
+    one box of 2^mbits particles and cells per side with the throughput box's
+    cell size (L = 500 Mpc/h at 512^3), spectrum and time step: one solver
+    state, one step per entry of `threads` (0: all host threads, the
+    reference's OpenMP default; 1: a single thread, on which its
+    `omp critical` deposit runs faster). Without oracle/_ref, one step of the
+    CPU restatement."""
+    import ctypes
+    n = 1 << mbits
+    L = L_BOX * n / 512
+    phi = _reference_potential(mbits, L)
+    R = _reference_lib()
+    per = {}
+    if R is not None:
+        allthreads = R.ref_max_threads()
+        th = (ctypes.c_int * len(threads))(*threads)
+        sec = (ctypes.c_double * len(threads))()
+        t_init = R.ref_time_threads(3, n, 1, ctypes.c_double(L), ctypes.c_double(68.5), ctypes.c_double(1.0),
+                                    ctypes.c_double(0.0), phi.ctypes.data_as(ctypes.c_void_p), ctypes.c_double(A0),
+                                    ctypes.c_double(DA), len(threads), th, sec)
+        for t, x in zip(threads, sec):
+            per[allthreads if t == 0 else t] = x
         kind = "reference"
-        while total < max_seconds and (max_steps is None or steps < max_steps):
-            t_init = ctypes.c_double()
-            dt = R.ref_time_steps(3, n, 1, ctypes.c_double(L), ctypes.c_double(68.5), ctypes.c_double(1.0),
-                                  ctypes.c_double(0.0), phi.ctypes.data_as(ctypes.c_void_p), ctypes.c_double(A0),
-                                  ctypes.c_double(DA), 1, ctypes.byref(t_init))
-            total += dt
-            steps += 1
     else:
-        kind = "port"
-        cores = 1
+        from oracle import cpu as oracle
         X, P = oracle.zeldovich(3, n, L, phi, A0, A0 + DA / 2)
-        a = A0
-        while total < max_seconds and (max_steps is None or steps < max_steps):
-            t0 = time.perf_counter()
-            oracle.drift(3, n, 68.5, 1.0, 0.0, X, P, a, DA)
-            oracle.kick(3, n, 1, L, 68.5, 1.0, 0.0, X, P, a + DA / 2, DA)
-            total += time.perf_counter() - t0
-            a += DA
-            steps += 1
-    value = n ** 3 * steps / total
-    return {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": kind,
-            "sample": f"{steps} leapfrog step(s) of a {n}^3-particle/{n}^3-mesh box, L={L:g} Mpc/h "
-                      f"(cell size of the 512^3 box), ns={NS}, from a={A0}; reference FP64 CPU code, "
-                      f"{cores} OpenMP threads", "seconds": total, "steps": steps}
+        t0 = time.perf_counter()
+        oracle.drift(3, n, 68.5, 1.0, 0.0, X, P, A0, DA)
+        oracle.kick(3, n, 1, L, 68.5, 1.0, 0.0, X, P, A0 + DA / 2, DA)
+        per[os.cpu_count()] = time.perf_counter() - t0
+        t_init, kind = None, "port"
+    best = min(per, key=per.get)
+    what = "reference FP64 CPU code" if kind == "reference" else "CPU restatement of the reference (FP64)"
+    return {"value": n ** 3 / per[best], "unit": "particle-steps/s", "cores": best, "kind": kind,
+            "sample": f"one leapfrog step (drift + kick) of a {n}^3-particle/{n}^3-mesh box, L={L:g} Mpc/h, "
+                      f"ns={NS}, from a={A0}, per thread count; {what}; value = the faster thread count",
+            "seconds_per_step_by_threads": {str(k): v for k, v in sorted(per.items())},
+            "init_seconds": t_init, "steps": 1, "seconds": per[best]}
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
-    for _ in range(args.warmup):
-        pass  # the reference has no JIT or caches to warm; warm-up steps are not timed
-    r = cpu_reference(max_seconds=1e9, max_steps=max(1, args.steps))
+    # One reference step of the full box takes minutes on the host cores, so
+    # a step here is one leapfrog step of the same box (all threads, then one
+    # thread, on one solver state); the warm-up steps have no counterpart (no
+    # JIT or caches to warm).
+    r = cpu_reference(mbits=args.mbits)
     line = {"metric": METRIC, "value": r["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
-            "steps": r["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / r["steps"],
+            "steps": r["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded mt19937 white noise, scale-free GRF)", "impl": "reference",
             "config": {"workload": workload_name(args.mbits, args.f), "sample": r["sample"]},
             "cpu_baseline": {"value": r["value"], "unit": r["unit"], "cores": r["cores"], "kind": r["kind"],
-                             "sample": r["sample"]},
+                             "sample": r["sample"], "seconds_per_step_by_threads": r["seconds_per_step_by_threads"]},
             "e2e": {"value": r["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def oracle_parity(cb, dev):
+    """FP32 GPU runs against the FP64 CPU oracle (the reference's algorithm)
+    on the same white noise, as checks beside the CPU baseline:
+    the 3D 128^3 box (L = 100, n_s = -2 smoothed at one cell, 50 steps from
+    a = 0.02) and the 32^3 class of the 96-box ensemble (32 boxes, 40 steps)."""
+    import numpy as np
+    from oracle import cpu as oracle
+    out = {}
+    N, mb, L = 128, 7, 100.0
+    noise = oracle.noise_mt19937(2, N ** 3)
+    phi = oracle.potential(3, mb, L, oracle.grf_scale_free(3, mb, L, -2.0, True, 0.78125, 0.83, noise))
+    Xr, _ = oracle.run(3, N, 1, L, 68.5, 1.0, 0.0, phi, 0.02, 0.0196, 50)
+    _, Pkr, cr = oracle.power_spectrum(3, N, L, oracle.md_cic(3, N, L, Xr) - 1.0)
+    g = cb.Gravity(3, N, 1, L, precision="fp32", device=dev)
+    g.run(phi, 0.02, 0.0196, 50)
+    X, _ = g.state()
+    _, Pk, _ = g.power_spectrum(len(cr))
+    g.close()
+    d = (X - Xr) / (L / N)
+    d = (d + N / 2) % N - N / 2
+    m = (cr > 0) & (np.arange(len(cr)) > 0)
+    out["c2_3d_128_fp32_vs_oracle"] = {
+        "position_rms_cells": float(np.sqrt(np.mean(d ** 2))), "position_max_cells": float(np.abs(d).max()),
+        "pk_ratio_max_abs_dev": float(np.max(np.abs(Pk[m] / Pkr[m] - 1))), "shells": int(m.sum()),
+        "what": "ic -d 3 -b 7 -L 100 --scale-free -n -2 --smooth --scale 0.78125 --seed 2; run -a0 0.02 "
+                "-da 0.0196 -n 50; FP32 GPU vs FP64 CPU oracle, same mt19937 noise and potential"}
+    from conan_b200.ensemble import Ensemble, standard_members
+    members = standard_members()[:32]
+    e = Ensemble(members, precision="fp32", device=dev)
+    e.init()
+    e.run()
+    gp = np.array([e.power_spectrum(i, 17)[1] for i in range(32)])
+    e.close()
+    rp = []
+    for mb5, Lm, ns, seed in members:
+        nz = cb.white_noise({"dim": 3, "mbits": mb5, "seed": seed}, device=dev)
+        ph = oracle.potential(3, mb5, Lm, oracle.grf_scale_free(3, mb5, Lm, ns, False, 8.0, 0.83, nz))
+        Xm, _ = oracle.run(3, 1 << mb5, 1, Lm, 68.5, 1.0, 0.0, ph, 0.05, 0.95 / 40, 40)
+        rp.append(oracle.power_spectrum(3, 1 << mb5, Lm, oracle.md_cic(3, 1 << mb5, Lm, Xm) - 1.0, 17)[1])
+    rp = np.array(rp)
+    out["c5_ensemble_32_class_fp32_vs_oracle"] = {
+        "mean_pk_max_rel_err": float(np.max(np.abs(gp.mean(0)[1:] / rp.mean(0)[1:] - 1))),
+        "worst_member_pk_max_rel_err": float(np.max(np.abs(gp[:, 1:] / rp[:, 1:] - 1))),
+        "what": "32 boxes of 32^3 (ns from default_rng(6), seeds 1000+i), 40 steps a=0.05->1, batched FP32 run "
+                "vs FP64 CPU oracle on the same white noise"}
+    return out
 
 
 # ------------------------------------------------------------------- ours --
@@ -389,6 +453,51 @@ def dram_traffic(kernel, workload):
     except OSError:
         pass
     return None
+
+
+def fd_check(dev, eps_list=(1e-3, 1e-4, 1e-5), nvox=64):
+    """Central finite differences of the differentiable 128^3 box's loss
+    (mean squared difference of the final density to that of seed 1004, 32
+    steps a = 0.05 -> 1, checkpoint 8) on 64 voxels of the white noise
+    (numpy default_rng(5)), FP64 forward, against the FP64 adjoint: relative
+    error per voxel, median / 90th percentile / max for each step eps."""
+    import numpy as np
+    import torch
+    import conan_b200 as cb
+    from conan_b200.autograd import DiffPM
+    m = DiffPM(dim=3, mbits=7, L_box=100.0, ns=-2.0, a0=0.05, da=0.95 / 32, n=32, checkpoint_every=8,
+               precision="fp64", device=dev)
+    w = torch.tensor(cb.white_noise({"dim": 3, "mbits": 7, "seed": 4}, device=dev), device=f"cuda:{dev}")
+    wt = torch.tensor(cb.white_noise({"dim": 3, "mbits": 7, "seed": 1004}, device=dev), device=f"cuda:{dev}")
+    out = torch.empty(m.ncells, dtype=torch.float64, device=f"cuda:{dev}")
+    m.forward_raw(wt, out)
+    target = out.clone()
+
+    def loss(x):
+        m.forward_raw(x, out)
+        return float(((out - target) ** 2).mean())
+
+    loss(w)
+    g = torch.empty_like(w)
+    m.backward_raw((2 * (out - target) / m.ncells).contiguous(), g)
+    g = g.cpu().numpy()
+    idx = np.random.default_rng(5).choice(w.numel(), nvox, replace=False)
+    res = {}
+    for eps in eps_list:
+        rel = []
+        for i in idx:
+            wp, wm = w.clone(), w.clone()
+            wp[i] += eps
+            wm[i] -= eps
+            fd = (loss(wp) - loss(wm)) / (2 * eps)
+            rel.append(abs(g[i] - fd) / max(abs(fd), 1e-30))
+        rel = np.array(rel)
+        res[f"{eps:g}"] = {"median_rel_err": float(np.median(rel)), "p90_rel_err": float(np.percentile(rel, 90)),
+                           "max_rel_err": float(rel.max())}
+    m.close()
+    res["what"] = ("central FD of the loss on 64 voxels (default_rng(5)), FP64 forward, vs FP64 adjoint; "
+                   "128^3 box, L=100, ns=-2, 32 steps a=0.05->1, checkpoint 8")
+    return res
 
 
 def run_ours(args):
@@ -546,13 +655,21 @@ def run_ours(args):
     Ph = torch.empty((Np, 3), dtype=torch.float64).pin_memory().numpy()
     g = cb.Gravity(3, n, f, L_BOX, precision="fp32", device=dev)
     g.run(ph, A0, DA, args.warmup)
+    g.state_into(Xh, Ph)
     barrier(dist)
     torch.cuda.synchronize()
+    # every call is synchronous: host timestamps between them split the total
     t0 = time.perf_counter()
-    g.run(ph, A0, DA, args.steps)
-    g.state_into(Xh, Ph)
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+    g.init(ph, A0, A0 + DA / 2)  # potential upload (1 GB FP64) + Zel'dovich start
+    t1 = time.perf_counter()
+    g.run(None, A0, DA, args.steps)  # the K steps (one CUDA graph)
+    t2 = time.perf_counter()
+    g.state_into(Xh, Ph)  # FP64 X and P to host memory (6.4 GB)
+    t3 = time.perf_counter()
+    e2e_s = max_over_ranks(t3 - t0, dist)
+    breakdown = {"init_upload_zeldovich_s": t1 - t0, "steps_s": t2 - t1, "state_out_s": t3 - t2,
+                 "link_floor_s": phi.nbytes / (link["h2d_gbs"] * 1e9) + (Xh.nbytes + Ph.nbytes) /
+                 (link["d2h_gbs"] * 1e9)}
     g.close()
 
     # the cic tool on the final snapshot (host positions in, host density out)
@@ -585,11 +702,9 @@ def run_ours(args):
 
     adjoint = None
     if not args.no_adjoint and rank == 0:
-        try:
-            from conan_b200 import autograd as ag
-            adjoint = ag.benchmark_adjoint_ratio(device=dev)
-        except (ImportError, AttributeError, NotImplementedError):
-            adjoint = None
+        from conan_b200 import autograd as ag
+        adjoint = ag.benchmark_adjoint_ratio(device=dev)
+        adjoint["finite_differences"] = fd_check(dev)
 
     ensemble = None
     if not args.no_ensemble and rank == 0:
@@ -620,9 +735,14 @@ def run_ours(args):
                     "tuning": tuning}
         e.close()
 
-    cpu = None
+    # CPU leg (rank 0, N = 1): the reference's own step on a bounded sample of
+    # the box (256^3 particles and cells with the same cell size, one step on
+    # one thread: about half a minute on the host cores), and the oracle
+    # parity checks of the FP32 path
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference()
+        cpu = cpu_reference(mbits=min(mbits, 8), threads=(1,))
+        parity = oracle_parity(cb, dev)
 
     if rank == 0:
         value = world * Np * args.steps / (ms32 * 1e-3)
@@ -650,9 +770,11 @@ def run_ours(args):
             "e2e": {"value": world * Np * args.steps / e2e_s, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": phi.nbytes / args.steps,
                     "d2h_bytes_per_step": (Xh.nbytes + Ph.nbytes) / args.steps,
-                    "what": "conan_pm_run (potential upload, Zel'dovich init, K steps) + conan_pm_get_state",
-                    "seconds": e2e_s, "host_link": link},
+                    "what": "conan_pm_init (potential upload, Zel'dovich start) + conan_pm_run (K steps) + "
+                            "conan_pm_get_state, pinned host buffers",
+                    "seconds": e2e_s, "breakdown": breakdown, "host_link": link},
             "cpu_baseline": cpu,
+            "oracle_parity": parity,
             "clocks": clocks,
             "remeasured": remeasured,
         }

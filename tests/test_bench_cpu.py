@@ -35,8 +35,10 @@ def test_dram_traffic_of_the_dominant_kernel_is_committed(bench):
 
 
 def test_reference_arm_prints_one_json_line():
-    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"],
-                       cwd=ROOT, capture_output=True, text=True, timeout=600)
+    # a 64^3 box keeps the reference's two timed steps short here (the
+    # default is the full 512^3 box)
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0",
+                        "--mbits", "6"], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -48,6 +50,8 @@ def test_reference_arm_prints_one_json_line():
     assert d["value"] > 0 and d["unit"] == "particle-steps/s" and d["higher_is_better"] is True
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    if d["cpu_baseline"]["kind"] == "reference":  # one step at all threads and one at a single thread
+        assert "1" in d["cpu_baseline"]["seconds_per_step_by_threads"]
 
 
 class _FakeNVML:
