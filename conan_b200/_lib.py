@@ -98,6 +98,7 @@ SIGNATURES = {
     "conan_pm_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "conan_pm_sync": (C.c_int, [C.c_void_p]),
     "conan_pm_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "conan_pm_autotune": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_char_p, C.c_size_t]),
     "conan_diff_create": (C.c_void_p, [C.POINTER(DiffParams)]),
     "conan_diff_destroy": (None, [C.c_void_p]),
     "conan_diff_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

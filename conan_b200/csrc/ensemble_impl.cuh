@@ -6,8 +6,9 @@
 // batched solver (every kernel launch covers all its members, cuFFT runs
 // batched), and each class runs on its own stream. conan_ens_run launches one
 // CUDA graph that holds the whole n-step run of every class, the classes on
-// parallel branches. An autotuner times the deposit's tile/block variants
-// per class on the class's initial state and keeps the fastest.
+// parallel branches. The solver's autotuner picks the deposit and
+// gradient-mesh kernels per class on the class's state half way through the
+// run (clustered), then the initial state is restored.
 #pragma once
 
 #include <chrono>
@@ -52,7 +53,7 @@ template <typename T, int R> struct Ens : EnsBase {
         T *noise = nullptr, *tnoise = nullptr, *target = nullptr, *dens = nullptr, *gd = nullptr, *gn = nullptr;
         T *s0[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
         cudaEvent_t join = nullptr, t0 = nullptr, t1 = nullptr;
-        double tune_ms[DEP_VARIANTS + 1] = {0, 0, 0, 0};  // sorted tiles, then Lagrangian (-1: not run)
+        double tune_a = 0;  // scale factor of the state the autotuner timed (0: not tuned)
     };
     conan_ens_params prm{};
     std::vector<conan_ens_member> mem;
@@ -176,30 +177,16 @@ template <typename T, int R> struct Ens : EnsBase {
         return CONAN_OK;
     }
 
-    // Times each deposit variant that fits (3 launches after a warm-up).
+    // Autotunes the class on a clustered state: the members are run half
+    // way (n/2 steps from their initial state), the solver's autotuner times
+    // its knobs there, and the initial state is put back.
     int tune(Cls &c) {
         auto &pm = c.d->pm;
-        double best = 1e30;
-        int bv = 0;
-        c.tune_ms[DEP_VARIANTS] = -1;
-        const int nv = pm.lag_v >= 0 && pm.lacc ? DEP_VARIANTS + 1 : DEP_VARIANTS;
-        for (int v = 0; v < nv; ++v) {
-            pm.dep_variant = v;
-            CONAN_TRY(pm.deposit());
-            CONAN_CUDA(cudaEventRecord(c.t0, pm.st));
-            for (int r = 0; r < 3; ++r) CONAN_TRY(pm.deposit());
-            CONAN_CUDA(cudaEventRecord(c.t1, pm.st));
-            CONAN_CUDA(cudaEventSynchronize(c.t1));
-            float ms = 0;
-            CONAN_CUDA(cudaEventElapsedTime(&ms, c.t0, c.t1));
-            c.tune_ms[v] = ms / 3;
-            if (ms < best) {
-                best = ms;
-                bv = v;
-            }
-        }
-        pm.dep_variant = bv;
-        return CONAN_OK;
+        double a = prm.a0;
+        CONAN_TRY(pm.steps(a, prm.da, 0, std::max(1u, prm.n / 2)));
+        CONAN_TRY(pm.tune(a, prm.da));
+        c.tune_a = a;
+        return load_state(c);
     }
 
     int init() override {
@@ -350,12 +337,12 @@ template <typename T, int R> struct Ens : EnsBase {
             const auto &c = cls[i];
             char buf[256];
             snprintf(buf, sizeof buf,
-                     "%s{\"mesh\": %d, \"L\": %g, \"members\": %zu, \"deposit_variant\": %d, "
-                     "\"deposit\": \"%s\", \"tune_ms\": [%.4f, %.4f, %.4f, %.4f]}",
-                     i ? ", " : "", 1 << c.mbits, c.L, c.members.size(), c.d->pm.dep_variant,
-                     c.d->pm.lag_on() ? "lagrangian" : "sorted", c.tune_ms[0], c.tune_ms[1], c.tune_ms[2],
-                     c.tune_ms[3]);
+                     "%s{\"mesh\": %d, \"L\": %g, \"members\": %zu, \"deposit\": \"%s\", \"tuned_at_a\": %g, "
+                     "\"tuning\": ",
+                     i ? ", " : "", 1 << c.mbits, c.L, c.members.size(), c.d->pm.lag_on() ? "lagrangian" : "sorted",
+                     c.tune_a);
             s += buf;
+            s += c.d->pm.tune_report() + "}";
         }
         s += "]}";
         return s;

@@ -317,6 +317,7 @@ template <typename T, int R> struct PM : PMBase {
     size_t tma_smem = 0;
 
     int tma_setup() {
+        tma_ok = false;
         if constexpr (sizeof(T) == 4 && R == 3) {
             typedef LagTile<3, 0> L;
             const char *off = getenv("CONAN_NO_TMA");
@@ -568,9 +569,195 @@ template <typename T, int R> struct PM : PMBase {
     // Packed FD4 gradient mesh of phi. (Measured at 512^3: the plain
     // thread-per-cell kernel beats four-cells-per-thread and warp-shuffle
     // variants, 0.64 against 0.68 and 0.83 ms.)
+    // Gradient-mesh kernel: z-marching tiles (3D, 32 cells per side and
+    // more) or one thread per cell in blocks of grad_block threads; the
+    // autotuner picks one.
+    bool grad_zm = FD_GRAD_ZM != 0;
+    int grad_block = 256;
+    bool grad_zm_fits() const { return R == 3 && mf.n >= 32; }
+
     int fd_gradient(const T *phi, G4<T> *g) {
+        if constexpr (R == 3) {
+            if (grad_zm && grad_zm_fits()) {
+                const unsigned blocks = (unsigned)((size_t)(mf.n / 32) * (mf.n / 8) * (mf.n / FDZ_PLANES) * mf.batch);
+                CONAN_TIMED(prof, "fd_grad", st, (k_fd_grad_zm<T><<<blocks, 256, 0, st>>>(phi, g, mf)));
+                return CONAN_OK;
+            }
+        }
+        const unsigned bs = (unsigned)grad_block;
         CONAN_TIMED(prof, "fd_grad", st,
-                    (k_fd_grad<T, R><<<(unsigned)((mf.cells + 255) / 256), 256, 0, st>>>(phi, g, mf)));
+                    (k_fd_grad<T, R><<<(unsigned)((mf.cells + bs - 1) / bs), bs, 0, st>>>(phi, g, mf)));
+        return CONAN_OK;
+    }
+
+    // --- autotuner -----------------------------------------------------------
+    // On the current particle state (a clustered one: tile costs grow as the
+    // particles cluster) it chooses (1) the deposit: the sorted tile variants,
+    // the Lagrangian window tiles V0..V2 and the direct two-cell window
+    // (FP32); (2) the gradient-mesh kernel: one thread per cell in blocks of
+    // 128, 256 or 512, or z-marching tiles. Knobs are tuned one after the
+    // other; each candidate runs one untimed and TUNE_STEPS timed leapfrog
+    // steps (CUDA events) from a copy of the state, which is restored at the
+    // end.
+    struct TuneRec {
+        std::string knob, value;
+        double ms;  // per timed step
+        bool chosen;
+    };
+    std::vector<TuneRec> tuned;
+    static constexpr int TUNE_STEPS = 2;
+    struct DepCand {
+        int mode;  // 0 sorted, 1 Lagrangian window, 2 Lagrangian direct
+        int v;
+        std::string name;
+    };
+
+    template <int V> bool dep_fits() const {
+        typedef DepTile<R, V> D;
+        return mf.n >= D::TX && mf.n >= D::TY && mf.n >= D::TZ;
+    }
+    bool lag_set(int v, bool direct) {
+        return v == 0 ? lag_try<0>(direct) : v == 1 ? lag_try<1>(direct) : lag_try<2>(direct);
+    }
+    int dep_apply(const DepCand &c) {
+        CONAN_TRY(drop_lag_deposit());
+        if (c.mode == 0) {
+            dep_variant = c.v;
+            return CONAN_OK;
+        }
+        if (!lag_set(c.v, c.mode == 2)) return set_error(CONAN_ERR_STATE, "deposit candidate %s no longer fits", c.name.c_str());
+        dep_variant = DEP_LAG;
+        return tma_setup();
+    }
+
+    // Time of one timed leapfrog step from the saved state.
+    int tune_time(T *const *save, double a, double da, double *ms) {
+        for (int k = 0; k < R; ++k) {
+            CONAN_CUDA(cudaMemcpyAsync(P.d[k], save[k], np * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            CONAN_CUDA(cudaMemcpyAsync(P.p[k], save[R + k], np * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        CONAN_TRY(positions_reset());
+        double aa = a;
+        CONAN_TRY(steps(aa, da, 0, 1));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CONAN_CUDA(cudaEventCreate(&e0));
+        CONAN_CUDA(cudaEventCreate(&e1));
+        cudaEventRecord(e0, st);
+        int rc = steps(aa, da, 1, 1 + TUNE_STEPS);
+        cudaEventRecord(e1, st);
+        cudaError_t se = cudaEventSynchronize(e1);
+        float t = 0;
+        if (se == cudaSuccess) se = cudaEventElapsedTime(&t, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rc != CONAN_OK) return rc;
+        if (se != cudaSuccess) return set_error(CONAN_ERR_CUDA, "autotuner timing: %s", cudaGetErrorString(se));
+        *ms = t / TUNE_STEPS;
+        return check_err();
+    }
+
+    int tune(double a, double da) {
+        tuned.clear();
+        const double apos = a_pos, amom = a_mom;
+        std::vector<T *> save(2 * R, nullptr);
+        for (auto &b : save) CONAN_CUDA(cudaMalloc(&b, np * sizeof(T)));
+        for (int k = 0; k < R; ++k) {
+            CONAN_CUDA(cudaMemcpyAsync(save[k], P.d[k], np * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            CONAN_CUDA(cudaMemcpyAsync(save[R + k], P.p[k], np * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        const bool prof_was = prof.on;
+        prof.on = false;
+        int rc = tune_knobs(save.data(), a, da);
+        prof.on = prof_was;
+        for (int k = 0; k < R && rc == CONAN_OK; ++k) {
+            cudaMemcpyAsync(P.d[k], save[k], np * sizeof(T), cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(P.p[k], save[R + k], np * sizeof(T), cudaMemcpyDeviceToDevice, st);
+        }
+        cudaStreamSynchronize(st);
+        for (auto b : save) cudaFree(b);
+        if (rc != CONAN_OK) return rc;
+        CONAN_TRY(positions_reset());
+        mesh_holds = 0;
+        a_pos = apos;
+        a_mom = amom;
+        return CONAN_OK;
+    }
+
+    int tune_knobs(T *const *save, double a, double da) {
+        // (1) the deposit
+        std::vector<DepCand> cands;
+        if (dep_fits<0>()) cands.push_back({0, 0, "sorted 32x8x8 / 256 threads"});
+        if (dep_fits<1>()) cands.push_back({0, 1, "sorted 32x4x8 / 128 threads"});
+        if (dep_fits<2>()) cands.push_back({0, 2, "sorted 32x16x8 / 512 threads"});
+        if (sizeof(T) == 4 && lacc) {
+            const char *tile[3] = {"", "", ""};
+            if (R == 3) tile[0] = "32x8x8", tile[1] = "16x8x8", tile[2] = "8x8x8";
+            if (R == 2) tile[0] = "64x32", tile[1] = "32x16", tile[2] = "16x16";
+            if (R == 1) tile[0] = "2048", tile[1] = "512", tile[2] = "128";
+            for (int v = 0; v < 3; ++v)
+                if (lag_set(v, false)) cands.push_back({1, v, std::string("lagrangian window, tile ") + tile[v]});
+            for (int v = 0; v < 3; ++v)
+                if (lag_set(v, true)) {
+                    cands.push_back({2, v, std::string("lagrangian direct, tile ") + tile[v]});
+                    break;
+                }
+        }
+        int best = -1;
+        double bms = 1e30;
+        for (size_t i = 0; i < cands.size(); ++i) {
+            double ms = 0;
+            CONAN_TRY(dep_apply(cands[i]));
+            CONAN_TRY(tune_time(save, a, da, &ms));
+            tuned.push_back({"deposit", cands[i].name, ms, false});
+            if (ms < bms) bms = ms, best = (int)i;
+        }
+        if (best >= 0) {
+            CONAN_TRY(dep_apply(cands[best]));
+            tuned[tuned.size() - cands.size() + best].chosen = true;
+        }
+        // (2) the gradient mesh (FD4 only)
+        if (prm.gradient == CONAN_GRAD_FD4) {
+            struct GC { bool zm; int block; std::string name; };
+            std::vector<GC> g = {{false, 128, "thread per cell, 128"}, {false, 256, "thread per cell, 256"},
+                                 {false, 512, "thread per cell, 512"}};
+            if (grad_zm_fits()) g.push_back({true, 256, "z-marching 32x8 tiles"});
+            best = -1;
+            bms = 1e30;
+            for (size_t i = 0; i < g.size(); ++i) {
+                grad_zm = g[i].zm;
+                grad_block = g[i].block;
+                double ms = 0;
+                CONAN_TRY(tune_time(save, a, da, &ms));
+                tuned.push_back({"gradient", g[i].name, ms, false});
+                if (ms < bms) bms = ms, best = (int)i;
+            }
+            grad_zm = g[best].zm;
+            grad_block = g[best].block;
+            tuned[tuned.size() - g.size() + best].chosen = true;
+        }
+        return CONAN_OK;
+    }
+
+    std::string tune_report() const {
+        std::string s = "[";
+        for (size_t i = 0; i < tuned.size(); ++i) {
+            char buf[256];
+            snprintf(buf, sizeof buf, "%s{\"knob\": \"%s\", \"value\": \"%s\", \"ms_per_step\": %.4f, \"chosen\": %s}",
+                     i ? ", " : "", tuned[i].knob.c_str(), tuned[i].value.c_str(), tuned[i].ms,
+                     tuned[i].chosen ? "true" : "false");
+            s += buf;
+        }
+        return s + "]";
+    }
+
+    int autotune(double a, double da, char *report, size_t len) override {
+        CONAN_TRY(tune(a, da));
+        if (report && len) {
+            std::string r = tune_report();
+            std::strncpy(report, r.c_str(), len - 1);
+            report[len - 1] = 0;
+            if (r.size() >= len) return set_error(CONAN_ERR_ARG, "report buffer too small (%zu bytes needed)", r.size() + 1);
+        }
         return CONAN_OK;
     }
 
@@ -1071,6 +1258,11 @@ int conan_pm_device_bytes(conan_pm *h, size_t *bytes) {
 int conan_pm_sync(conan_pm *h) {
     H_GUARD(h);
     return h->impl->sync();
+}
+int conan_pm_autotune(conan_pm *h, double a, double da, char *report, size_t len) {
+    H_GUARD(h);
+    if (!(da > 0) || !(a > 0)) return set_error(CONAN_ERR_ARG, "need a > 0 and da > 0");
+    return h->impl->autotune(a, da, report, len);
 }
 int conan_pm_get_stream(conan_pm *h, void **stream) {
     H_GUARD(h);

@@ -40,6 +40,7 @@ struct PMBase {
     virtual int set_cb_every(unsigned k) = 0;
     virtual int set_deposit(int mode) = 0;
     virtual int get_deposit(int *mode) = 0;
+    virtual int autotune(double a, double da, char *report, size_t len) = 0;
     virtual int device() const = 0;
     virtual void *stream() const = 0;
 };

@@ -597,7 +597,7 @@ __device__ inline G4<double> load_g4(const G4<double> *p) {
 // the reference's Gradient<R>::operator[] (src/run/numeric.hh:88-100)
 // evaluated once per node for all particles that interpolate it.
 template <typename T, int R>
-__global__ void __launch_bounds__(256) k_fd_grad(const T *__restrict__ phi, G4<T> *__restrict__ G, Mesh m) {
+__global__ void __launch_bounds__(512) k_fd_grad(const T *__restrict__ phi, G4<T> *__restrict__ G, Mesh m) {
     uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.cells) return;
     const uint32_t mask = m.n - 1;
@@ -611,6 +611,60 @@ __global__ void __launch_bounds__(256) k_fd_grad(const T *__restrict__ phi, G4<T
         g[k] = (at(-2) - at(2)) * c12 + (at(1) - at(-1)) * c23;
     }
     G[c] = G4<T>{g[0], g[1], g[2], T(0)};
+}
+
+// The same gradient for 3D meshes of at least 32 cells per side, marching
+// along z: a CTA of 32 x 8 threads takes a 32 x 8 column of cells over FZ
+// planes. Each plane's tile with a two-cell halo in x and y is staged in
+// shared memory (two buffers, one barrier per plane) for the x and y
+// differences, and each thread keeps its column's five z values in
+// registers; the same arithmetic as k_fd_grad, so the same bits.
+#ifndef FD_GRAD_ZM
+#define FD_GRAD_ZM 0
+#endif
+constexpr int FDZ_PLANES = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fd_grad_zm(const T *__restrict__ phi, G4<T> *__restrict__ G, Mesh m) {
+    __shared__ T tile[2][12][36];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const uint32_t mask = (uint32_t)m.n - 1;
+    const int s = m.shift;
+    const int nbx = m.n >> 5, nby = m.n >> 3, nbz = m.n / FDZ_PLANES;
+    unsigned b = blockIdx.x;
+    const int bx = (int)(b % nbx);
+    b /= nbx;
+    const int by = (int)(b % nby);
+    b /= nby;
+    const int bz = (int)(b % nbz);
+    const size_t mb = (size_t)(b / nbz) << m.cshift;
+    const T *__restrict__ ph = phi + mb;
+    G4<T> *__restrict__ g = G + mb;
+    const int x0 = bx * 32, y0 = by * 8, z0 = bz * FDZ_PLANES;
+    auto at = [&](int xx, int yy, int zz) {
+        return __ldg(ph + (((size_t)((uint32_t)zz & mask) << (2 * s)) | (((uint32_t)yy & mask) << s) |
+                           ((uint32_t)xx & mask)));
+    };
+    const T c12 = T(1) / T(12), c23 = T(2) / T(3);
+    T q[5];  // this column at z - 2 .. z + 2
+#pragma unroll
+    for (int j = 0; j < 5; ++j) q[j] = at(x0 + tx, y0 + ty, z0 - 2 + j);
+    for (int zi = 0; zi < FDZ_PLANES; ++zi) {
+        const int z = z0 + zi;
+        T(*t)[36] = tile[zi & 1];
+        for (int e = threadIdx.x; e < 12 * 36; e += 256) {
+            const int r = e / 36, c = e - r * 36;
+            t[r][c] = at(x0 - 2 + c, y0 - 2 + r, z);
+        }
+        __syncthreads();
+        const T gx = (t[ty + 2][tx] - t[ty + 2][tx + 4]) * c12 + (t[ty + 2][tx + 3] - t[ty + 2][tx + 1]) * c23;
+        const T gy = (t[ty][tx + 2] - t[ty + 4][tx + 2]) * c12 + (t[ty + 3][tx + 2] - t[ty + 1][tx + 2]) * c23;
+        const T gz = (q[0] - q[4]) * c12 + (q[3] - q[1]) * c23;
+        g[((size_t)z << (2 * s)) | ((size_t)(y0 + ty) << s) | (size_t)(x0 + tx)] = G4<T>{gx, gy, gz, T(0)};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) q[j] = q[j + 1];
+        if (zi + 1 < FDZ_PLANES) q[4] = at(x0 + tx, y0 + ty, z + 3);
+    }
 }
 
 // CIC-interpolated force of particle i: sum over corners of weight times

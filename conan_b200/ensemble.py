@@ -104,7 +104,7 @@ class Ensemble:
         return n.value
 
     def describe(self) -> dict:
-        buf = C.create_string_buffer(8192)
+        buf = C.create_string_buffer(65536)
         L.check(L.lib().conan_ens_describe(self._h, buf, len(buf)))
         return json.loads(buf.value.decode())
 

@@ -326,6 +326,16 @@ class Gravity:
         L.check(L.lib().conan_pm_set_deposit(self._h, {"sorted": L.DEPOSIT_SORTED,
                                                        "lagrangian": L.DEPOSIT_LAGRANGIAN}[mode]))
 
+    def autotune(self, a: float, da: float) -> list:
+        """Times the deposit and gradient-mesh variants over leapfrog steps
+        from the current state (scale factor a of the next drift, step da)
+        and keeps the fastest; the state is left as it was. Returns the
+        timings: [{knob, value, ms_per_step, chosen}, ...]."""
+        import json
+        buf = C.create_string_buffer(16384)
+        L.check(L.lib().conan_pm_autotune(self._h, a, da, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def stream_ptr(self) -> int:
         """The handle's cudaStream_t as an integer (torch.cuda.ExternalStream)."""
         s = C.c_void_p()

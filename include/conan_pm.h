@@ -266,6 +266,18 @@ int conan_pm_sync(conan_pm *h);
 /* The handle's CUDA stream (a cudaStream_t), e.g. to record timing events
  * around library calls. */
 int conan_pm_get_stream(conan_pm *h, void **stream);
+/* Autotuner (no reference counterpart: the reference has one code path).
+ * On the handle's current particle state -- best a clustered one, e.g.
+ * half way through a run, since tile costs grow with clustering -- it times
+ * every fitting candidate of each knob over leapfrog steps from a copy of
+ * the state and keeps the fastest: the deposit (sorted tile variants;
+ * Lagrangian window tiles; the direct two-cell window) and the
+ * gradient-mesh kernel (thread per cell at 128/256/512 threads; z-marching
+ * tiles). a: scale factor of the next drift; da: the step. The state and
+ * scale factors are left as they were. `report` (may be NULL) receives a
+ * JSON list of {knob, value, ms_per_step, chosen}. Allocates a temporary
+ * copy of the particle state. */
+int conan_pm_autotune(conan_pm *h, double a, double da, char *report, size_t len);
 
 /* --------------------------------------------------------- adjoint -- */
 

@@ -46,8 +46,14 @@ def test_graph_run_repeats_and_autotuner_reports(gpu, conan):
     d = e.describe()
     assert len(d["classes"]) == 2
     for c in d["classes"]:
-        assert 0 <= c["deposit_variant"] <= 3  # 3: Lagrangian
         assert c["deposit"] in ("sorted", "lagrangian")
+        assert c["tuned_at_a"] > 0.05  # timed on the state half way through the run
+        knobs = {t["knob"] for t in c["tuning"]}
+        assert knobs == {"deposit", "gradient"}
+        for k in knobs:  # one chosen value per knob, the fastest timed
+            ts = [t for t in c["tuning"] if t["knob"] == k]
+            chosen = [t for t in ts if t["chosen"]]
+            assert len(chosen) == 1 and chosen[0]["ms_per_step"] == min(t["ms_per_step"] for t in ts)
     assert e.total_particles() == 3 * 32 ** 3 + 2 * 16 ** 3
     e.close()
 
@@ -72,3 +78,33 @@ def test_ensemble_mean_pk_is_finite(gpu, conan):
     k, P = e.mean_power_spectrum(8)
     assert np.all(np.isfinite(P)) and np.all(P[1:] > 0)
     e.close()
+
+
+def test_single_box_autotuner_keeps_state_and_results(gpu, conan):
+    """The solver's autotuner on a clustered 64^3 state: every knob reports
+    its candidates, the state comes back unchanged, and the run after tuning
+    gives the density of an untuned solver (the deposit variants sum the same
+    integers, the gradient variants do the same arithmetic; the sorted and
+    Lagrangian paths gather in different kernels, so FP32 rounding of the
+    later steps may differ)."""
+    n, L = 64, 64.0
+    H = {"dim": 3, "mbits": 6, "size": L, "ns": -2.0, "smooth": 0, "scale-free": 1, "scale": 8.0, "sigma": 0.83,
+         "seed": 9}
+    phi = conan.compute_potential(H, conan.generate_random_field(H))
+    a0, da = 0.05, 0.05
+    out = []
+    for tuned in (False, True):
+        g = conan.Gravity(3, n, 1, L, precision="fp32")
+        g.run(phi, a0, da, 8)
+        X0, P0 = g.state()
+        if tuned:
+            rep = g.autotune(a0 + 8 * da, da)
+            X1, P1 = g.state()
+            assert np.array_equal(X0, X1) and np.array_equal(P0, P1)
+            assert {r["knob"] for r in rep} == {"deposit", "gradient"}
+            assert sum(r["chosen"] for r in rep) == 2
+        g.run(None, a0 + 8 * da, da, 4)
+        out.append(g.density())
+        g.close()
+    assert np.max(np.abs(out[0] - out[1])) <= 1e-5 * max(1.0, np.max(np.abs(out[0])))
+
