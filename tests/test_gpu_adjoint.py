@@ -150,7 +150,8 @@ def test_fp32_adjoint_on_the_differentiable_box_against_the_cpu_adjoint(gpu, con
           f"components above 1% of the largest ({big.sum()}): median rel {np.median(rel):.2e}, 99th pct "
           f"{np.percentile(rel, 99):.2e}, max {rel.max():.2e}; cosine {cos:.9f}; FP32 final density max err "
           f"{dens_err:.2e} of max")
-    assert rel_max < 5e-3 and np.median(rel) < 1e-3
+    # measured on a B200: 5.9e-4 of the largest component, median 1.8e-4
+    assert rel_max < 2e-3 and np.median(rel) < 5e-4
 
 
 def test_finite_differences_on_the_differentiable_box(gpu, conan):
@@ -191,10 +192,14 @@ def test_finite_differences_on_the_differentiable_box(gpu, conan):
     m.close()
     # The CIC deposit and gather are piecewise linear in the positions: a
     # finite difference whose step moves particles across cell faces sees the
-    # kinks, an error that shrinks in proportion to eps, while the adjoint
-    # gives the derivative itself.
-    assert np.median(res[1e-5]) < 1e-4 and np.mean(res[1e-5] < 1e-3) > 0.9
-    assert np.median(res[1e-3]) < 1e-2
+    # kinks. The share of particles within eps of a face and the error each
+    # of them adds both grow with eps, so the finite-difference error falls
+    # about as eps^2 (measured on a B200, median: 9.0e-4, 4.0e-6, 8.0e-7 at
+    # eps = 1e-3, 1e-4, 1e-5), while the adjoint gives the derivative itself.
+    assert np.median(res[1e-5]) < 1e-5 and np.mean(res[1e-5] < 1e-4) > 0.9
+    assert np.median(res[1e-4]) < 1e-4
+    assert np.median(res[1e-3]) < 2e-3
+    assert np.median(res[1e-3]) > 30 * np.median(res[1e-4])  # the kinks' signature
 
 
 def test_adjoint_cost_at_most_three_forwards(gpu, conan):
