@@ -319,41 +319,50 @@ template <typename T, int R> struct PM : PMBase {
     int tma_setup() {
         tma_ok = false;
         if constexpr (sizeof(T) == 4 && R == 3) {
-            typedef LagTile<3, 0> L;
             const char *off = getenv("CONAN_NO_TMA");
-            if ((off && *off && *off != '0') || lag_v != 0) return CONAN_OK;
-            typedef CUresult (*Encode)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                       const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
-                                       CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                                       CUtensorMapFloatOOBfill);
-            void *fn = nullptr;
-            cudaDriverEntryPointQueryResult q{};
-            if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-                !fn) {
-                cudaGetLastError();
-                return CONAN_OK;  // no encoder: the kernel reads global memory directly
-            }
-            const cuuint64_t n = (cuuint64_t)mm.n;
-            const cuuint64_t dims[3] = {n, n, n * (cuuint64_t)mm.batch};
-            const cuuint64_t strides[2] = {n * 4, n * n * 4};
-            // one group of z-planes: one particle per thread of the tile
-            const cuuint32_t box[3] = {L::LX, L::LY, L::THREADS / (L::LX * L::LY)}, estr[3] = {1, 1, 1};
-            float *arr[6] = {P.d[0], P.d[1], P.d[2], P.p[0], P.p[1], P.p[2]};
-            for (int a = 0; a < 6; ++a)
-                if (((Encode)fn)(&tmaps.a[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, arr[a], dims, strides, box, estr,
-                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-                    return CONAN_OK;
-            const size_t stage_bytes = (size_t)(6 * L::LX * L::LY * L::LZ * 4 + 128);
-            // the window after the staged arrays, or over them
-            tma_smem = LAG_STAGE_KEEP ? stage_bytes + lag_smem : std::max(lag_smem, stage_bytes);
-            auto kern = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem) != cudaSuccess) {
-                cudaGetLastError();
-                return CONAN_OK;
-            }
-            tma_ok = true;
+            if (off && *off && *off != '0') return CONAN_OK;
+            if (lag_v == 0) return tma_setup_v<0>();
+            if (lag_v == 1) return tma_setup_v<1>();
+            if (lag_v == 2) return tma_setup_v<2>();
         }
+        return CONAN_OK;
+    }
+
+    // Tensor maps over d[k], p[k] with the box of one particle group of
+    // lattice tile V (LX x LY x THREADS / (LX LY)), and the staged kernel's
+    // shared memory; tma_ok stays false when anything is missing (the
+    // kernels then read global memory directly).
+    template <int V> int tma_setup_v() {
+        typedef LagTile<3, V> L;
+        typedef CUresult (*Encode)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn) {
+            cudaGetLastError();
+            return CONAN_OK;
+        }
+        const cuuint64_t n = (cuuint64_t)mm.n;
+        const cuuint64_t dims[3] = {n, n, n * (cuuint64_t)mm.batch};
+        const cuuint64_t strides[2] = {n * 4, n * n * 4};
+        // one group of z-planes: one particle per thread of the tile
+        const cuuint32_t box[3] = {L::LX, L::LY, L::THREADS / (L::LX * L::LY)}, estr[3] = {1, 1, 1};
+        float *arr[6] = {P.d[0], P.d[1], P.d[2], P.p[0], P.p[1], P.p[2]};
+        for (int a = 0; a < 6; ++a)
+            if (((Encode)fn)(&tmaps.a[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, arr[a], dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return CONAN_OK;
+        const size_t stage_bytes = (size_t)(6 * L::LX * L::LY * L::LZ * 4 + 128);
+        // the window after the staged arrays, or over them
+        tma_smem = LAG_STAGE_KEEP ? stage_bytes + lag_smem : std::max(lag_smem, stage_bytes);
+        auto kern = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem) != cudaSuccess) {
+            cudaGetLastError();
+            return CONAN_OK;
+        }
+        tma_ok = true;
         return CONAN_OK;
     }
 
@@ -362,9 +371,10 @@ template <typename T, int R> struct PM : PMBase {
             typedef LagTile<R, V> L;
             size_t tiles = (size_t)(mm.n / L::LX) * (R >= 2 ? mm.n / L::LY : 1) * (R == 3 ? mm.n / L::LZ : 1) *
                            (size_t)mm.batch;
-            if constexpr (R == 3 && V == 0) {
-                // staged drift+deposit: 1.87 against 2.33 ms at 512^3; with the
-                // gather the direct loads win (3.76 against 3.82 ms)
+            if constexpr (R == 3) {
+                // staged (512^3, 32x8x8 tiles): drift+deposit 1.87 against 2.33
+                // ms; with the gather, keeping the drifted displacements in the
+                // staged memory and a one-plane window 3.55 against 3.76 ms
                 if (tma_ok && (LAG_TMA_GATHER || !c.kick)) {
                     auto tk = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
                     CONAN_TIMED(prof, name, st,

@@ -806,9 +806,12 @@ struct LagWin {
 // beyond the tile's own f*L cells, split over both sides) of variant V.
 constexpr int LAG_VARIANTS = 3;
 // 32-bit planes of a window cell: 2 keeps the carry in shared memory, 1
-// sends it to the accumulator mesh; a compile-time tunable.
+// sends it to the accumulator mesh (a carry needs over 2^9 particles' weight
+// in one cell of one tile: rare). A compile-time tunable; one plane leaves
+// room for the TMA-staged tile's arrays beside its window (3.55 against 3.76
+// ms per fused launch at 512^3).
 #ifndef LAG_PLANES
-#define LAG_PLANES 2
+#define LAG_PLANES 1
 #endif
 
 // Window cells per particle of a tile above which the deposit goes to the
@@ -894,15 +897,15 @@ __device__ __forceinline__ void gather_g4(const G4<float> *__restrict__ Gm, int 
 
 // Staged tiles keep the drifted displacements in the staging memory and
 // place the window after it (instead of over it): the deposit reads the
-// particles back from shared memory, not from registers. A compile-time
-// tunable.
+// particles back from shared memory, not from registers, and the window is
+// cleared while the copies arrive. A compile-time tunable.
 #ifndef LAG_STAGE_KEEP
-#define LAG_STAGE_KEEP 0
+#define LAG_STAGE_KEEP 1
 #endif
 // The gather + kick + drift + deposit launches staged too (not only the
 // first drift + deposit); a compile-time tunable.
 #ifndef LAG_TMA_GATHER
-#define LAG_TMA_GATHER 0
+#define LAG_TMA_GATHER 1
 #endif
 
 template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED, bool STAGED = false>
