@@ -346,8 +346,8 @@ template <typename T, int R> struct PM : PMBase {
         const cuuint64_t n = (cuuint64_t)mm.n;
         const cuuint64_t dims[3] = {n, n, n * (cuuint64_t)mm.batch};
         const cuuint64_t strides[2] = {n * 4, n * n * 4};
-        // one group of z-planes: one particle per thread of the tile
-        const cuuint32_t box[3] = {L::LX, L::LY, L::THREADS / (L::LX * L::LY)}, estr[3] = {1, 1, 1};
+        // one z-plane of the tile per copy
+        const cuuint32_t box[3] = {L::LX, L::LY, 1}, estr[3] = {1, 1, 1};
         float *arr[6] = {P.d[0], P.d[1], P.d[2], P.p[0], P.p[1], P.p[2]};
         for (int a = 0; a < 6; ++a)
             if (((Encode)fn)(&tmaps.a[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, arr[a], dims, strides, box, estr,

@@ -918,6 +918,14 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
     constexpr int NW = THREADS / 32;
+    // Each thread takes NPT particles that follow each other along the
+    // tile's slowest axis (z in 3D), so that one particle's upper corners can
+    // meet the next one's lower corners in registers (see the deposit);
+    // lanes of a warp take consecutive x, so loads stay coalesced.
+    constexpr int NS = R == 3 ? LZ : R == 2 ? LY : LX;  // tile cells along the slowest axis
+    constexpr int PL = NT / NS;                          // particles per layer of that axis
+    static_assert(THREADS % PL == 0 && (THREADS / PL) * NPT == NS, "threads must cover whole layers");
+    auto tidx = [](int j) { return (((int)threadIdx.x / PL) * NPT + j) * PL + (int)threadIdx.x % PL; };
     constexpr bool KEEP = STAGED && LAG_STAGE_KEEP;
     extern __shared__ __align__(16) uint32_t lag_dyn[];
     uint32_t *lag_sh = KEEP ? reinterpret_cast<uint32_t *>(stage + 6 * NT) : lag_dyn;  // the window
@@ -956,7 +964,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
-        const int t = (int)threadIdx.x + j * THREADS;
+        const int t = tidx(j);
         const int lx = t % LX, ly = (t / LX) % LY, lz = t / (LX * LY);
         const int c[3] = {tx0 + lx, ty0 + ly, tz0 + lz};
         uint32_t i = (uint32_t)c[0];
@@ -1056,13 +1064,40 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
 
     const int o0 = org[0], o1 = R >= 2 ? org[1] : 0, o2 = R == 3 ? org[2] : 0;
     const int W0 = win.w[0], W1 = win.w[1], W2 = win.w[2], W01 = W0 * W1;
+    constexpr int NB = 1 << R, HALF = NB / 2;  // corners; the upper half has the slowest axis' bit set
+    // global cell of corner b of a particle in (unwrapped) cell uc
+    auto corner_g = [&](const int *uc, int b) {
+        uint32_t g = (uint32_t)(uc[0] + (b & 1)) & mask;
+        if (R >= 2) g |= ((uint32_t)(uc[1] + ((b >> 1) & 1)) & mask) << m.shift;
+        if (R == 3) g |= ((uint32_t)(uc[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
+        return g;
+    };
+    auto woff = [&](int b) { return (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W01; };
+    // adds v into window cell wc (corner b of a particle in cell uc)
+    auto win_add = [&](int wc, uint32_t v, const int *uc, int b) {
+        if constexpr (LAG_PLANES == 2) {
+            Slot<float>::add(lag_sh, wc, v, cells);
+        } else if (v) {
+            // one plane: a carry out of the 32-bit cell goes to the
+            // accumulator mesh directly (rare: over 2^9 particles' weight)
+            const uint32_t old = atomicAdd(lag_sh + wc, v);
+            if (old + v < old) atomicAdd(accm + corner_g(uc, b), 1ull << 32);
+        }
+    };
+    // the upper corners of this thread's previous particle, held back while
+    // they may coincide with the next particle's lower corners (the next
+    // particle one cell further along the slowest axis): their integer
+    // weights are then added in registers before one window add
+    bool pend = false;
+    int pu[3] = {0, 0, 0}, pwc = 0;
+    uint32_t pw[HALF];
 #pragma unroll
     for (int j = 0; j < NPT; ++j) {
         // cells (unwrapped) and 21-bit fractions of the deposit position
-        int u[3];
+        int u[3] = {0, 0, 0};
         uint32_t fr[3];
         {
-            const int t = (int)threadIdx.x + j * THREADS;
+            const int t = tidx(j);
             const int c[3] = {tx0 + t % LX, ty0 + (t / LX) % LY, tz0 + t / (LX * LY)};
 #pragma unroll
             for (int k = 0; k < R; ++k) {
@@ -1083,38 +1118,44 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             wz[0] = 1.0f - f2;
             wz[1] = f2;
         }
+        uint32_t v[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) v[b] = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
         const int l0 = u[0] - o0, l1 = R >= 2 ? u[1] - o1 : 0, l2 = R == 3 ? u[2] - o2 : 0;
         const bool inside = l0 >= 0 && l0 + 1 < W0 && (R < 2 || (l1 >= 0 && l1 + 1 < W1)) &&
                             (R < 3 || (l2 >= 0 && l2 + 1 < W2));
+        if (pend) {
+            bool meet = inside && u[R - 1] == pu[R - 1] + 1;
+#pragma unroll
+            for (int k = 0; k < R - 1; ++k) meet = meet && u[k] == pu[k];
+            if (meet) {
+#pragma unroll
+                for (int h = 0; h < HALF; ++h) v[h] += pw[h];  // <= 2^24: no overflow
+            } else {
+#pragma unroll
+                for (int h = 0; h < HALF; ++h) win_add(pwc + woff(HALF + h), pw[h], pu, HALF + h);
+            }
+            pend = false;
+        }
         if (inside) {
             const int base = (l2 * W1 + l1) * W0 + l0;
 #pragma unroll
-            for (int b = 0; b < (1 << R); ++b) {
-                uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                const int wc = base + (b & 1) + ((b >> 1) & 1) * W0 + ((b >> 2) & 1) * W01;
-                if constexpr (LAG_PLANES == 2) {
-                    Slot<float>::add(lag_sh, wc, v, cells);
-                } else if (v) {
-                    // one plane: a carry out of the 32-bit cell goes to the
-                    // accumulator mesh directly (rare: over 2^9 particles' weight)
-                    const uint32_t old = atomicAdd(lag_sh + wc, v);
-                    if (old + v < old) {
-                        uint32_t g = (uint32_t)(u[0] + (b & 1)) & mask;
-                        if (R >= 2) g |= ((uint32_t)(u[1] + ((b >> 1) & 1)) & mask) << m.shift;
-                        if (R == 3) g |= ((uint32_t)(u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
-                        atomicAdd(accm + g, 1ull << 32);
-                    }
-                }
+            for (int h = 0; h < HALF; ++h) win_add(base + woff(h), v[h], u, h);
+            if (j + 1 < NPT) {
+                pend = true;
+                pwc = base;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) pu[k] = u[k];
+#pragma unroll
+                for (int h = 0; h < HALF; ++h) pw[h] = v[HALF + h];
+            } else {
+#pragma unroll
+                for (int h = 0; h < HALF; ++h) win_add(base + woff(HALF + h), v[HALF + h], u, HALF + h);
             }
         } else {
 #pragma unroll
-            for (int b = 0; b < (1 << R); ++b) {
-                uint32_t v = quant_w(wx[b & 1] * wy[(b >> 1) & 1] * wz[(b >> 2) & 1]);
-                uint32_t g = (uint32_t)(u[0] + (b & 1)) & mask;
-                if (R >= 2) g |= ((uint32_t)(u[1] + ((b >> 1) & 1)) & mask) << m.shift;
-                if (R == 3) g |= ((uint32_t)(u[2] + ((b >> 2) & 1)) & mask) << (2 * m.shift);
-                if (v) atomicAdd(accm + g, (unsigned long long)v);
-            }
+            for (int b = 0; b < NB; ++b)
+                if (v[b]) atomicAdd(accm + corner_g(u, b), (unsigned long long)v[b]);
         }
     }
     __syncthreads();
@@ -1167,8 +1208,9 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 // ------------------------------------------- TMA staging of a 3D tile --
 //
 // The six particle arrays of a 3D lattice tile (d[0..2], p[0..2], LX x LY x
-// LZ floats each) come from tensor maps over the (N, N, N*batch) arrays, in
-// NPT groups of LZ/NPT z-planes: group j holds every thread's particle j.
+// LZ floats each, in tile order) come from tensor maps over the (N, N,
+// N*batch) arrays, one z-plane per bulk tensor copy, in NPT groups: group j
+// holds every thread's particle j (the planes s NPT + j).
 // Thread 0 issues the bulk tensor copies of all groups at once, each group
 // completing its own mbarrier, and every thread waits for group j just
 // before it needs particle j, so the first particles are computed while the
@@ -1178,7 +1220,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
 // deposits nothing. No multicast: every copy reads this GPU's own memory into
 // this CTA.
 struct TileMaps {
-    CUtensorMap a[6];  // d0, d1, d2, p0, p1, p2; box LX x LY x (LZ / NPT)
+    CUtensorMap a[6];  // d0, d1, d2, p0, p1, p2; box LX x LY x 1
 };
 
 __device__ inline uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -1202,8 +1244,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
     k_gkd_lag_tma(Parts<float> P, Mesh m, const G4<float> *__restrict__ G, GKD gc, LagWin win,
                   unsigned long long *__restrict__ acc, const __grid_constant__ TileMaps maps, int *err) {
     static_assert(R == 3, "the staged tile is three-dimensional");
-    constexpr int NT = LX * LY * LZ, NPT = NT / THREADS, GZ = LZ / NPT;
-    static_assert(GZ * NPT == LZ && GZ * LX * LY == THREADS, "a group of z-planes holds one particle per thread");
+    constexpr int NT = LX * LY * LZ, NPT = NT / THREADS, GP = THREADS / (LX * LY);
+    static_assert(GP * NPT == LZ && GP * LX * LY == THREADS, "a group of z-planes holds one particle per thread");
     extern __shared__ __align__(16) uint32_t lag_sh[];
     __shared__ __align__(8) unsigned long long bars[NPT];
     __shared__ int stage_fail;
@@ -1228,13 +1270,18 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
             const uint32_t b = smem_addr(bars + j);
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(6u * THREADS * 4u)
                          : "memory");
+            // group j: the planes s NPT + j, one box (LX x LY x 1) each
 #pragma unroll
             for (int a = 0; a < 6; ++a)
-                asm volatile(
-                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                    " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(stage + a * NT + j * THREADS)),
-                    "l"(reinterpret_cast<uint64_t>(&maps.a[a])), "r"(x0), "r"(y0), "r"(z0 + j * GZ), "r"(b)
-                    : "memory");
+#pragma unroll
+                for (int q = 0; q < GP; ++q) {
+                    const int lz = q * NPT + j;
+                    asm volatile(
+                        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(stage + a * NT + lz * LX * LY)),
+                        "l"(reinterpret_cast<uint64_t>(&maps.a[a])), "r"(x0), "r"(y0), "r"(z0 + lz), "r"(b)
+                        : "memory");
+                }
         }
     }
     lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage, bars, err, &stage_fail);
