@@ -52,6 +52,25 @@ int set_error(int code, const char *fmt, ...);
                                       cudaGetErrorString(e_), __FILE__, __LINE__);         \
     } while (0)
 
+// Raises (never lowers) kernel kern's limit of dynamic shared memory to at
+// least `bytes`. The limit belongs to the kernel function, not to a handle:
+// lowering it for one handle's launch configuration would make another
+// handle's larger launch of the same kernel fail. False when the device
+// cannot give that much (the error state is cleared).
+template <typename K> bool raise_dyn_smem(K kern, size_t bytes) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return true;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
 inline bool is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
 inline int ilog2(long long n) {
     int s = 0;

@@ -284,11 +284,7 @@ template <typename T, int R> struct PM : PMBase {
         if constexpr (sizeof(T) == 4) {  // set once here, outside any stream capture
             auto kern = k_deposit_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
             auto fused = k_gkd_lag<R, L::LX, L::LY, L::LZ, L::THREADS>;
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess ||
-                cudaFuncSetAttribute(fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess) {
-                cudaGetLastError();
-                return false;
-            }
+            if (!raise_dyn_smem(kern, sh) || !raise_dyn_smem(fused, sh)) return false;
         }
         lwin = w;
         lag_smem = sh;
@@ -358,10 +354,7 @@ template <typename T, int R> struct PM : PMBase {
         // the window after the staged arrays, or over them
         tma_smem = LAG_STAGE_KEEP ? stage_bytes + lag_smem : std::max(lag_smem, stage_bytes);
         auto kern = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem) != cudaSuccess) {
-            cudaGetLastError();
-            return CONAN_OK;
-        }
+        if (!raise_dyn_smem(kern, tma_smem)) return CONAN_OK;
         tma_ok = true;
         return CONAN_OK;
     }
@@ -377,9 +370,16 @@ template <typename T, int R> struct PM : PMBase {
                 // staged memory and a one-plane window 3.55 against 3.76 ms
                 if (tma_ok && (LAG_TMA_GATHER || !c.kick)) {
                     auto tk = k_gkd_lag_tma<3, L::LX, L::LY, L::LZ, L::THREADS>;
-                    CONAN_TIMED(prof, name, st,
-                                (tk<<<(unsigned)tiles, L::THREADS, tma_smem, st>>>(P, mf, grad, c, lwin, lacc,
-                                                                                   tmaps, err)));
+                    const int rec = prof.begin(name, st);
+                    tk<<<(unsigned)tiles, L::THREADS, tma_smem, st>>>(P, mf, grad, c, lwin, lacc, tmaps, err);
+                    cudaError_t e = cudaGetLastError();
+                    if (e != cudaSuccess)
+                        return set_error(CONAN_ERR_CUDA,
+                                         "staged launch failed: %s (tile %dx%dx%d, %d threads, %zu tiles, %zu bytes "
+                                         "shared, window %d cells)",
+                                         cudaGetErrorString(e), L::LX, L::LY, L::LZ, L::THREADS, tiles, tma_smem,
+                                         lwin.cells);
+                    prof.end(rec, st);
                     return CONAN_OK;
                 }
             }
