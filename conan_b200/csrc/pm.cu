@@ -192,6 +192,8 @@ template <typename T, int R> struct PM : PMBase {
             CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st));
             dep_variant = DEP_LAG;
             CONAN_TRY(tma_setup());
+            pers = LAG_PERSIST != 0;
+            CONAN_TRY(pers_setup());
         }
         CONAN_TRY(fft.create(mf, sizeof(T) == 8, batch));
         size_t wbytes = fft.work_bytes;
@@ -359,11 +361,57 @@ template <typename T, int R> struct PM : PMBase {
         return CONAN_OK;
     }
 
+    // Persistent staged launch (3D, lattice tiles 32x8x8 and 16x8x8 with twice
+    // the threads, two staging buffers): on when `pers` and its set-up
+    // succeeded for the current tile variant.
+    bool pers = false, pers_ok = false;
+    unsigned pers_grid = 0;
+    size_t pers_smem = 0;
+    template <int V> struct PersT {
+        typedef LagTile<3, V> L;
+        static constexpr int THREADS = 2 * L::THREADS;
+    };
+    int pers_setup() {
+        pers_ok = false;
+        if constexpr (sizeof(T) == 4 && R == 3) {
+            if (!pers || !tma_ok || lag_v > 1) return CONAN_OK;
+            return lag_v == 0 ? pers_setup_v<0>() : pers_setup_v<1>();
+        }
+        return CONAN_OK;
+    }
+    template <int V> int pers_setup_v() {
+        typedef LagTile<3, V> L;
+        constexpr int TH = PersT<V>::THREADS;
+        auto kern = k_gkd_lag_pers<3, L::LX, L::LY, L::LZ, TH>;
+        pers_smem = 128 + 2 * 6 * (size_t)(L::LX * L::LY * L::LZ) * 4 + lag_smem;
+        if (!raise_dyn_smem(kern, pers_smem)) return CONAN_OK;
+        int nb = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TH, pers_smem) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, prm.device) != cudaSuccess || nb < 1) {
+            cudaGetLastError();
+            return CONAN_OK;
+        }
+        pers_grid = (unsigned)(nb * sms);
+        pers_ok = true;
+        return CONAN_OK;
+    }
+
     template <int V> int launch_gkd_lag(const GKD &c, const char *name) {
         if constexpr (sizeof(T) == 4) {
             typedef LagTile<R, V> L;
             size_t tiles = (size_t)(mm.n / L::LX) * (R >= 2 ? mm.n / L::LY : 1) * (R == 3 ? mm.n / L::LZ : 1) *
                            (size_t)mm.batch;
+            if constexpr (R == 3 && V <= 1) {
+                if (pers_ok && tma_ok && (LAG_TMA_GATHER || !c.kick)) {
+                    constexpr int TH = PersT<V>::THREADS;
+                    auto pk = k_gkd_lag_pers<3, L::LX, L::LY, L::LZ, TH>;
+                    const unsigned grid = (unsigned)std::min<size_t>(pers_grid, tiles);
+                    CONAN_TIMED(prof, name, st,
+                                (pk<<<grid, TH, pers_smem, st>>>(P, mf, grad, c, lwin, lacc, tmaps, err,
+                                                                  (unsigned)tiles)));
+                    return CONAN_OK;
+                }
+            }
             if constexpr (R == 3) {
                 // staged (512^3, 32x8x8 tiles): drift+deposit 1.87 against 2.33
                 // ms; with the gather, keeping the drifted displacements in the
@@ -617,7 +665,7 @@ template <typename T, int R> struct PM : PMBase {
     std::vector<TuneRec> tuned;
     static constexpr int TUNE_STEPS = 2;
     struct DepCand {
-        int mode;  // 0 sorted, 1 Lagrangian window, 2 Lagrangian direct
+        int mode;  // 0 sorted, 1 Lagrangian window, 2 Lagrangian direct, 3 Lagrangian window, persistent
         int v;
         std::string name;
     };
@@ -631,13 +679,15 @@ template <typename T, int R> struct PM : PMBase {
     }
     int dep_apply(const DepCand &c) {
         CONAN_TRY(drop_lag_deposit());
+        pers = c.mode == 3;
         if (c.mode == 0) {
             dep_variant = c.v;
             return CONAN_OK;
         }
         if (!lag_set(c.v, c.mode == 2)) return set_error(CONAN_ERR_STATE, "deposit candidate %s no longer fits", c.name.c_str());
         dep_variant = DEP_LAG;
-        return tma_setup();
+        CONAN_TRY(tma_setup());
+        return pers_setup();
     }
 
     // Time of one timed leapfrog step from the saved state.
@@ -706,6 +756,10 @@ template <typename T, int R> struct PM : PMBase {
             if (R == 1) tile[0] = "2048", tile[1] = "512", tile[2] = "128";
             for (int v = 0; v < 3; ++v)
                 if (lag_set(v, false)) cands.push_back({1, v, std::string("lagrangian window, tile ") + tile[v]});
+            if (R == 3)
+                for (int v = 0; v < 2; ++v)
+                    if (lag_set(v, false))
+                        cands.push_back({3, v, std::string("lagrangian window, tile ") + tile[v] + ", persistent"});
             for (int v = 0; v < 3; ++v)
                 if (lag_set(v, true)) {
                     cands.push_back({2, v, std::string("lagrangian direct, tile ") + tile[v]});

@@ -838,7 +838,7 @@ template <> struct LagTile<1, 2> { static constexpr int LX = 128, LY = 1, LZ = 1
 // STAGED: the tile's d[0..2], p[0..2] arrive in shared memory (six
 // LX*LY*LZ arrays in tile order, see k_gkd_lag_tma), particle group j
 // signalled by bars[j]; otherwise they are read from global memory.
-__device__ inline bool tma_wait(unsigned long long *bar, unsigned limit);
+__device__ inline bool tma_wait(unsigned long long *bar, unsigned limit, unsigned parity = 0);
 constexpr unsigned TMA_WAIT_LIMIT = 1u << 20;  // polls of try_wait (about a second at most)
 
 // Deposit position of a displacement d (force cells) along one axis: d
@@ -902,18 +902,30 @@ __device__ __forceinline__ void gather_g4(const G4<float> *__restrict__ Gm, int 
 #ifndef LAG_STAGE_KEEP
 #define LAG_STAGE_KEEP 1
 #endif
+// The staged fused launches run as persistent CTAs that prefetch their next
+// tile (k_gkd_lag_pers) by default; a compile-time tunable, and a knob of
+// the autotuner.
+#ifndef LAG_PERSIST
+#define LAG_PERSIST 0
+#endif
 // The gather + kick + drift + deposit launches staged too (not only the
 // first drift + deposit); a compile-time tunable.
 #ifndef LAG_TMA_GATHER
 #define LAG_TMA_GATHER 1
 #endif
 
-template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED, bool STAGED = false>
+// PERSIST: one tile of a persistent CTA (k_gkd_lag_pers): the tile index,
+// the phase parity of this use of the staging buffer's barriers and the
+// window (kept clear between tiles: the flush zeroes what it reads) come
+// from the caller.
+template <int R, int LX, int LY, int LZ, int THREADS, bool FUSED, bool STAGED = false, bool PERSIST = false>
 __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, const LagWin &win,
                                          unsigned long long *__restrict__ acc, const G4<float> *__restrict__ G,
                                          const GKD &gc, float *stage = nullptr,
                                          unsigned long long *bars = nullptr, int *err = nullptr,
-                                         int *stage_fail = nullptr) {
+                                         int *stage_fail = nullptr, unsigned btile = 0, unsigned parity = 0,
+                                         uint32_t *wsh = nullptr) {
+    static_assert(!PERSIST || (STAGED && FUSED), "a persistent tile is staged and fused");
     constexpr int NT = LX * LY * LZ;
     constexpr int NPT = LX * LY * LZ / THREADS;  // particles per thread
     static_assert(NPT * THREADS == LX * LY * LZ, "tile must be a multiple of the block");
@@ -928,11 +940,11 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     auto tidx = [](int j) { return (((int)threadIdx.x / PL) * NPT + j) * PL + (int)threadIdx.x % PL; };
     constexpr bool KEEP = STAGED && LAG_STAGE_KEEP;
     extern __shared__ __align__(16) uint32_t lag_dyn[];
-    uint32_t *lag_sh = KEEP ? reinterpret_cast<uint32_t *>(stage + 6 * NT) : lag_dyn;  // the window
+    uint32_t *lag_sh = PERSIST ? wsh : KEEP ? reinterpret_cast<uint32_t *>(stage + 6 * NT) : lag_dyn;  // the window
     __shared__ int wred[6][NW];
     __shared__ int org[6];  // window origin per axis, then the extent of the box to flush
     const int cells = win.cells;
-    if constexpr (KEEP) {  // the window is free from the start: clear it while the copies arrive
+    if constexpr (KEEP && !PERSIST) {  // the window is free from the start: clear it while the copies arrive
         uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
         for (int c = threadIdx.x; c < cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
     }
@@ -940,7 +952,8 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     const int s = P.mshift;
     const int ntx = (1 << s) / LX, nty = R >= 2 ? (1 << s) / LY : 1, ntz = R == 3 ? (1 << s) / LZ : 1;
     const unsigned tiles = (unsigned)(ntx * nty * ntz);
-    const unsigned member = blockIdx.x / tiles, tile = blockIdx.x % tiles;
+    const unsigned bid = PERSIST ? btile : blockIdx.x;
+    const unsigned member = bid / tiles, tile = bid % tiles;
     const int tx0 = (int)(tile % ntx) * LX;
     const int ty0 = R >= 2 ? (int)((tile / ntx) % nty) * LY : 0;
     const int tz0 = R == 3 ? (int)(tile / (ntx * nty)) * LZ : 0;
@@ -977,7 +990,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             for (int k = 0; k < R; ++k) {  // read once: evict-first, L1 stays for the gradients
                 if constexpr (STAGED) {
                     // group j holds this thread's particle j
-                    if (k == 0 && !tma_wait(bars + j, TMA_WAIT_LIMIT)) {
+                    if (k == 0 && !tma_wait(bars + j, TMA_WAIT_LIMIT, parity)) {
                         atomicOr(err, 8);
                         *stage_fail = 1;
                     }
@@ -1036,7 +1049,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             // a copy did not arrive in time: wait (bounded again) for the
             // copies still in flight into this memory, then deposit nothing
             if (threadIdx.x == 0)
-                for (int j = 0; j < NPT; ++j) tma_wait(bars + j, TMA_WAIT_LIMIT);
+                for (int j = 0; j < NPT; ++j) tma_wait(bars + j, TMA_WAIT_LIMIT, parity);
             __syncthreads();
             return;
         }
@@ -1170,6 +1183,10 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
     for (int c = threadIdx.x; c < ecells; c += THREADS) {
         const int wc = (l2 * W1 + l1) * W0 + l0;
         uint32_t a = lag_sh[wc], b = LAG_PLANES == 2 ? lag_sh[cells + wc] : 0u;
+        if constexpr (PERSIST) {  // leave the window clear for the next tile
+            lag_sh[wc] = 0u;
+            if (LAG_PLANES == 2) lag_sh[cells + wc] = 0u;
+        }
         if (a | b) {
             uint32_t g = (uint32_t)(o0 + l0) & mask;
             if (R >= 2) g |= ((uint32_t)(o1 + l1) & mask) << m.shift;
@@ -1225,16 +1242,16 @@ struct TileMaps {
 
 __device__ inline uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Waits for phase 0 of mbarrier `bar`, at most `limit` polls; false when
-// the wait ran out.
-__device__ inline bool tma_wait(unsigned long long *bar, unsigned limit) {
+// Waits for the completion of the phase of parity `parity` of mbarrier
+// `bar`, at most `limit` polls; false when the wait ran out.
+__device__ inline bool tma_wait(unsigned long long *bar, unsigned limit, unsigned parity) {
     const uint32_t b = smem_addr(bar);
     uint32_t done = 0;
     for (unsigned it = 0; it < limit && !done; ++it)
         asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
             : "=r"(done)
-            : "r"(b)
+            : "r"(b), "r"(parity)
             : "memory");
     return done != 0;
 }
@@ -1285,6 +1302,82 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS)
         }
     }
     lag_tile<R, LX, LY, LZ, THREADS, true, true>(P, m, win, acc, G, gc, stage, bars, err, &stage_fail);
+}
+
+// Persistent form of the staged fused launch: a CTA loops over tiles t,
+// t + gridDim.x, ... and, while it works on one tile, the bulk tensor copies
+// of its next tile land in a second staging buffer, so the particle stream
+// never waits for a tile's start. Two buffers of the six arrays (one
+// mbarrier per particle group and buffer; use k of a buffer completes phase
+// k), then the window, which is cleared once here and kept clear by the
+// flush of every tile. Waits are bounded as in k_gkd_lag_tma; after one runs
+// out the CTA waits (bounded) for its copies in flight and stops.
+template <int R, int LX, int LY, int LZ, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+    k_gkd_lag_pers(Parts<float> P, Mesh m, const G4<float> *__restrict__ G, GKD gc, LagWin win,
+                   unsigned long long *__restrict__ acc, const __grid_constant__ TileMaps maps, int *err,
+                   unsigned ntiles) {
+    static_assert(R == 3, "the staged tile is three-dimensional");
+    constexpr int NT = LX * LY * LZ, NPT = NT / THREADS, GP = THREADS / (LX * LY);
+    static_assert(GP * NPT == LZ && GP * LX * LY == THREADS, "a group of z-planes holds one particle per thread");
+    extern __shared__ __align__(16) uint32_t lag_dyn[];
+    __shared__ __align__(8) unsigned long long bars[2][NPT];
+    __shared__ int stage_fail;
+    float *stage0 = reinterpret_cast<float *>((reinterpret_cast<uintptr_t>(lag_dyn) + 127) & ~(uintptr_t)127);
+    float *stage1 = stage0 + 6 * NT;
+    uint32_t *wsh = reinterpret_cast<uint32_t *>(stage1 + 6 * NT);
+    const int s = P.mshift;
+    const int ntx = (1 << s) / LX, nty = (1 << s) / LY, ntz = (1 << s) / LZ;
+    const unsigned tiles = (unsigned)(ntx * nty * ntz);
+    if (threadIdx.x == 0) {
+        stage_fail = 0;
+        for (int q = 0; q < 2 * NPT; ++q)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[0][0] + q)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    uint4 *z4 = reinterpret_cast<uint4 *>(wsh);
+    for (int c = threadIdx.x; c < win.cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    // thread 0: the copies of tile t into buffer q (group j: the planes
+    // g NPT + j of the tile, one box LX x LY x 1 each)
+    auto issue = [&](unsigned t, int q) {
+        const unsigned member = t / tiles, tile = t % tiles;
+        const int x0 = (int)(tile % ntx) * LX, y0 = (int)((tile / ntx) % nty) * LY;
+        const int z0 = (int)(tile / (ntx * nty)) * LZ + (int)(member << s);
+        float *st = q ? stage1 : stage0;
+        for (int j = 0; j < NPT; ++j) {
+            const uint32_t b = smem_addr(&bars[q][j]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(6u * THREADS * 4u)
+                         : "memory");
+#pragma unroll
+            for (int a = 0; a < 6; ++a)
+#pragma unroll
+                for (int g = 0; g < GP; ++g) {
+                    const int lz = g * NPT + j;
+                    asm volatile(
+                        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(st + a * NT + lz * LX * LY)),
+                        "l"(reinterpret_cast<uint64_t>(&maps.a[a])), "r"(x0), "r"(y0), "r"(z0 + lz), "r"(b)
+                        : "memory");
+                }
+        }
+    };
+    unsigned t = blockIdx.x;
+    if (threadIdx.x == 0 && t < ntiles) issue(t, 0);
+    for (unsigned it = 0; t < ntiles; t += gridDim.x, ++it) {
+        const int b = (int)(it & 1);
+        // the other buffer was last read by the previous tile's deposit,
+        // which every thread finished before that tile's flush
+        if (threadIdx.x == 0 && t + gridDim.x < ntiles) issue(t + gridDim.x, b ^ 1);
+        lag_tile<R, LX, LY, LZ, THREADS, true, true, true>(P, m, win, acc, G, gc, b ? stage1 : stage0, bars[b], err,
+                                                            &stage_fail, t, (it >> 1) & 1, wsh);
+        if (stage_fail) {  // set before a barrier inside lag_tile: the same for every thread
+            if (threadIdx.x == 0 && t + gridDim.x < ntiles)
+                for (int j = 0; j < NPT; ++j) tma_wait(&bars[b ^ 1][j], TMA_WAIT_LIMIT, ((it + 1) >> 1) & 1);
+            __syncthreads();
+            return;
+        }
+    }
 }
 
 // Density contrast from the integer accumulator (units of 2^-23 particle
