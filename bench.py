@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-cic", action="store_true")
     ap.add_argument("--no-fof", action="store_true")
     ap.add_argument("--no-mesh2", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (its trial launches), e.g. for a launch list")
     return ap.parse_args()
 
 
@@ -531,7 +532,7 @@ def run_ours(args):
         # then the autotuner on that state (it puts the state back)
         g.run(phi, A0, DA, args.warmup)
         g.sync()
-        tuning = g.autotune(A0 + args.warmup * DA, DA) if prec == "fp32" else None
+        tuning = g.autotune(A0 + args.warmup * DA, DA) if prec == "fp32" and not args.no_tune else None
         g.init(phi, A0, A0 + DA / 2)
         g.set_profiling(profile)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -659,7 +660,8 @@ def run_ours(args):
     Ph = torch.empty((Np, 3), dtype=torch.float64).pin_memory().numpy()
     g = cb.Gravity(3, n, f, L_BOX, precision="fp32", device=dev)
     g.run(ph, A0, DA, args.warmup)
-    g.autotune(A0 + args.warmup * DA, DA)
+    if not args.no_tune:
+        g.autotune(A0 + args.warmup * DA, DA)
     g.state_into(Xh, Ph)
     barrier(dist)
     torch.cuda.synchronize()

@@ -29,11 +29,14 @@ namespace conan {
 // Lines per CTA and threads per CTA for an n-point z transform: n / 8
 // threads per line. (At n = 1024, 4 lines per CTA instead of 8 measured
 // slower: 31.0 against 30.0 ms per step of the 1024^3-mesh run.)
-template <int N> struct ZTile {
-    static constexpr int TX = N >= 256 ? 8 : 2048 / N;
+// TX = 0 takes the default width; the autotuner also tries half and twice
+// the default (ZTile<N, TX>::OK says whether a width fits one CTA).
+template <int N, int TX_ = 0> struct ZTile {
+    static constexpr int TX = TX_ ? TX_ : (N >= 256 ? 8 : 2048 / N);
     static constexpr int LT = N / 8;  // threads per line
     static constexpr int THREADS = TX * LT;
     static constexpr size_t SMEM = (size_t)TX * N * sizeof(float2) + (size_t)N * sizeof(float2);
+    static constexpr bool OK = THREADS <= 1024 && SMEM <= 200 * 1024;
 };
 
 __device__ inline float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -118,9 +121,9 @@ struct ZGreen {
 // One Stockham stage of radix RAD with sub-length Ns. IN_G / OUT_G: read from
 // / write to global memory instead of shared memory; GREEN: multiply the
 // inputs by the Green's function first.
-template <int N, int RAD, bool INV, bool IN_G, bool OUT_G, bool GREEN>
+template <int N, int TXW, int RAD, bool INV, bool IN_G, bool OUT_G, bool GREEN>
 __device__ inline void zstage(const ZIO &io, int Ns, const float2 *tw, const ZGreen &gf) {
-    constexpr int TX = ZTile<N>::TX, LT = ZTile<N>::LT;
+    constexpr int TX = ZTile<N, TXW>::TX, LT = ZTile<N, TXW>::LT;
     constexpr int NB = N / RAD;  // butterflies per line
     constexpr int Q = NB / LT;   // butterflies per thread
     const int l = (int)threadIdx.x % TX, j0 = (int)threadIdx.x / TX;
@@ -183,13 +186,13 @@ template <int N> struct ZRadix {
 #define ZPASS_MIN_BLOCKS 3  // resident CTAs per SM the register budget must allow (measured: 0.45 against 0.51 ms with 1 at 512^3)
 #endif
 
-template <int N>
-__global__ void __launch_bounds__(ZTile<N>::THREADS, ZPASS_MIN_BLOCKS) k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
+template <int N, int TXW = 0>
+__global__ void __launch_bounds__(ZTile<N, TXW>::THREADS, ZPASS_MIN_BLOCKS) k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
                                                                    const float2 *__restrict__ twid) {
     extern __shared__ __align__(16) float2 zsh[];
-    constexpr int TX = ZTile<N>::TX;
+    constexpr int TX = ZTile<N, TXW>::TX;
     float2 *tw = zsh + TX * N;
-    for (int i = threadIdx.x; i < N; i += ZTile<N>::THREADS) tw[i] = twid[i];
+    for (int i = threadIdx.x; i < N; i += ZTile<N, TXW>::THREADS) tw[i] = twid[i];
     __syncthreads();
     const int kx0 = (int)blockIdx.x * TX, ky = (int)blockIdx.y;
     const size_t zs = (size_t)m.n * m.nh;
@@ -199,23 +202,23 @@ __global__ void __launch_bounds__(ZTile<N>::THREADS, ZPASS_MIN_BLOCKS) k_zpass_g
     constexpr int S8 = ZRadix<N>::S8, REST = ZRadix<N>::REST;
     // forward: radix-8 stages (the first from global memory), then the rest
     int Ns = 1;
-    zstage<N, 8, false, true, false, false>(io, Ns, tw, gf);
+    zstage<N, TXW, 8, false, true, false, false>(io, Ns, tw, gf);
     Ns *= 8;
 #pragma unroll
-    for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, 8, false, false, false, false>(io, Ns, tw, gf);
-    if constexpr (REST > 1) zstage<N, REST, false, false, false, false>(io, Ns, tw, gf);
+    for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, TXW, 8, false, false, false, false>(io, Ns, tw, gf);
+    if constexpr (REST > 1) zstage<N, TXW, REST, false, false, false, false>(io, Ns, tw, gf);
     // inverse, the Green's function applied as the first stage reads
     Ns = 1;
-    zstage<N, 8, true, false, false, true>(io, Ns, tw, gf);
+    zstage<N, TXW, 8, true, false, false, true>(io, Ns, tw, gf);
     Ns *= 8;
     if constexpr (REST > 1) {
 #pragma unroll
-        for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, 8, true, false, false, false>(io, Ns, tw, gf);
-        zstage<N, REST, true, false, true, false>(io, Ns, tw, gf);
+        for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, TXW, 8, true, false, false, false>(io, Ns, tw, gf);
+        zstage<N, TXW, REST, true, false, true, false>(io, Ns, tw, gf);
     } else {
 #pragma unroll
-        for (int s = 1; s < S8 - 1; ++s, Ns *= 8) zstage<N, 8, true, false, false, false>(io, Ns, tw, gf);
-        zstage<N, 8, true, false, true, false>(io, Ns, tw, gf);
+        for (int s = 1; s < S8 - 1; ++s, Ns *= 8) zstage<N, TXW, 8, true, false, false, false>(io, Ns, tw, gf);
+        zstage<N, TXW, 8, true, false, true, false>(io, Ns, tw, gf);
     }
 }
 

@@ -569,15 +569,50 @@ template <typename T, int R> struct PM : PMBase {
             default: return zpass_attr<1024>();
         }
     }
-    template <int N> int zpass_attr() {
-        CONAN_CUDA(cudaFuncSetAttribute(k_zpass_green<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)ZTile<N>::SMEM));
+    // z-pass lines per CTA: 0 the default width, else TX (the autotuner's knob)
+    int ztx = 0;
+    template <int N, int TX> int zpass_attr1() {
+        if constexpr (ZTile<N, TX>::OK)
+            if (!raise_dyn_smem(k_zpass_green<N, TX>, ZTile<N, TX>::SMEM))
+                return set_error(CONAN_ERR_CUDA, "z pass: %zu bytes of shared memory refused", ZTile<N, TX>::SMEM);
         return CONAN_OK;
     }
+    template <int N> int zpass_attr() {
+        constexpr int T0 = ZTile<N>::TX;
+        CONAN_TRY((zpass_attr1<N, 0>()));
+        CONAN_TRY((zpass_attr1<N, T0 / 2>()));
+        return zpass_attr1<N, 2 * T0>();
+    }
+    // widths of the z pass at this mesh size (default first)
+    std::vector<int> zpass_widths() const {
+        std::vector<int> w{0};
+        auto add = [&](auto tag) {
+            constexpr int N = decltype(tag)::value;
+            constexpr int T0 = ZTile<N>::TX;
+            if (ZTile<N, T0 / 2>::OK) w.push_back(T0 / 2);
+            if (ZTile<N, 2 * T0>::OK) w.push_back(2 * T0);
+        };
+        switch (mf.n) {
+            case 64: add(std::integral_constant<int, 64>()); break;
+            case 128: add(std::integral_constant<int, 128>()); break;
+            case 256: add(std::integral_constant<int, 256>()); break;
+            case 512: add(std::integral_constant<int, 512>()); break;
+            default: add(std::integral_constant<int, 1024>()); break;
+        }
+        return w;
+    }
+    template <int N, int TX> void zpass_launch1(float gs) {
+        if constexpr (ZTile<N, TX>::OK) {
+            typedef ZTile<N, TX> Z;
+            const dim3 grid((unsigned)((mf.nh + Z::TX - 1) / Z::TX), (unsigned)mf.n, (unsigned)mf.batch);
+            k_zpass_green<N, TX><<<grid, Z::THREADS, Z::SMEM, st>>>(reinterpret_cast<float2 *>(spec), mf, gs, ztw);
+        }
+    }
     template <int N> void zpass_launch(float gs) {
-        const dim3 grid((unsigned)((mf.nh + ZTile<N>::TX - 1) / ZTile<N>::TX), (unsigned)mf.n, (unsigned)mf.batch);
-        k_zpass_green<N><<<grid, ZTile<N>::THREADS, ZTile<N>::SMEM, st>>>(reinterpret_cast<float2 *>(spec), mf, gs,
-                                                                         ztw);
+        constexpr int T0 = ZTile<N>::TX;
+        if (ztx == T0 / 2 && ZTile<N, T0 / 2>::OK) zpass_launch1<N, T0 / 2>(gs);
+        else if (ztx == 2 * T0 && ZTile<N, 2 * T0>::OK) zpass_launch1<N, 2 * T0>(gs);
+        else zpass_launch1<N, 0>(gs);
     }
     // z FFT, Green multiply and inverse z FFT of the plane spectra (FP32)
     int green_z(double gs) {
@@ -798,6 +833,24 @@ template <typename T, int R> struct PM : PMBase {
             grad_zm = g[best].zm;
             grad_block = g[best].block;
             tuned[tuned.size() - g.size() + best].chosen = true;
+        }
+        // (3) the z pass's lines per CTA (FP32 3D plane-transform solve)
+        if (zpass) {
+            const std::vector<int> w = zpass_widths();
+            best = -1;
+            bms = 1e30;
+            for (size_t i = 0; i < w.size(); ++i) {
+                ztx = w[i];
+                double ms = 0;
+                CONAN_TRY(tune_time(save, a, da, &ms));
+                char nm[64];
+                if (w[i]) snprintf(nm, sizeof nm, "%d lines per CTA", w[i]);
+                else snprintf(nm, sizeof nm, "default lines per CTA");
+                tuned.push_back({"z pass", nm, ms, false});
+                if (ms < bms) bms = ms, best = (int)i;
+            }
+            ztx = w[best];
+            tuned[tuned.size() - w.size() + best].chosen = true;
         }
         return CONAN_OK;
     }

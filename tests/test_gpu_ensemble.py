@@ -101,8 +101,9 @@ def test_single_box_autotuner_keeps_state_and_results(gpu, conan):
             rep = g.autotune(a0 + 8 * da, da)
             X1, P1 = g.state()
             assert np.array_equal(X0, X1) and np.array_equal(P0, P1)
-            assert {r["knob"] for r in rep} == {"deposit", "gradient"}
-            assert sum(r["chosen"] for r in rep) == 2
+            knobs = {r["knob"] for r in rep}
+            assert knobs == {"deposit", "gradient", "z pass"}  # a 64^3 mesh solves Poisson with the z pass
+            assert sum(r["chosen"] for r in rep) == len(knobs)
         g.run(None, a0 + 8 * da, da, 4)
         out.append(g.density())
         g.close()
