@@ -900,6 +900,15 @@ template <typename T, int R> struct PM : PMBase {
             lag_ready = true;
             return CONAN_OK;
         }
+        // the last kick of a run (no drift, no deposit) on the same staged
+        // tiles instead of the thread-per-particle kernel
+        if (kick && !drift && !rank_after && lag_on() && prm.gradient == CONAN_GRAD_FD4) {
+            c.deposit = 0;
+            if (lag_v == 0) CONAN_TRY(launch_gkd_lag<0>(c, name));
+            else if (lag_v == 1) CONAN_TRY(launch_gkd_lag<1>(c, name));
+            else CONAN_TRY(launch_gkd_lag<2>(c, name));
+            return CONAN_OK;
+        }
         if (prm.gradient == CONAN_GRAD_SPECTRAL)
             CONAN_TIMED(prof, name, st,
                         (k_gkd<T, R, true><<<grid_p(), 256, 0, st>>>(P, mf, mesh, gm[0], gm[1], gm[2], grad, c,

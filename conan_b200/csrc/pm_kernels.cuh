@@ -740,6 +740,7 @@ struct GKD {
     double ck;  // kick: p -= F ck (0 disables)
     double cd;  // drift: d += p cd (after the kick)
     int kick, drift, rank, periodic;
+    int deposit = 1;  // fused Lagrangian tiles: deposit the drifted positions (0: kick and/or drift only)
 };
 
 // Fused leapfrog update of particle i: the kick of Gravity::kick
@@ -1012,12 +1013,14 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
                     __stcs(pm[k] + i, p[k]);
                 }
             }
-            const float cd = (float)gc.cd;
+            if (gc.drift) {
+                const float cd = (float)gc.cd;
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                d[k] += p[k] * cd;
-                __stcs(dm[k] + i, d[k]);
-                if constexpr (KEEP) stage[k * NT + t] = d[k];
+                for (int k = 0; k < R; ++k) {
+                    d[k] += p[k] * cd;
+                    __stcs(dm[k] + i, d[k]);
+                    if constexpr (KEEP) stage[k * NT + t] = d[k];
+                }
             }
         } else {
 #pragma unroll
@@ -1054,6 +1057,7 @@ __device__ __forceinline__ void lag_tile(const Parts<float> &P, const Mesh &m, c
             return;
         }
     }
+    if (!gc.deposit) return;  // a kick-only launch (the last of a run): no deposit
     if constexpr (!KEEP) {
         uint4 *z4 = reinterpret_cast<uint4 *>(lag_sh);
         for (int c = threadIdx.x; c < cells * LAG_PLANES / 4; c += THREADS) z4[c] = make_uint4(0u, 0u, 0u, 0u);
