@@ -113,8 +113,8 @@ struct ZGreen {
     float gs;
     __device__ inline float operator()(int e, int l) const {
         const int kz = e > n / 2 ? e - n : e;
-        const long long k2 = (long long)(kx0 + l) * (kx0 + l) + kyy + (long long)kz * kz;
-        return k2 > 0 ? gs / (float)k2 : 0.0f;
+        const int k2 = (kx0 + l) * (kx0 + l) + (int)kyy + kz * kz;  // <= 3 (n/2)^2: fits 32 bits
+        return k2 > 0 ? __fdividef(gs, (float)k2) : 0.0f;
     }
 };
 
