@@ -400,8 +400,7 @@ template <typename T, int R> struct Diff : DiffBase {
             if (i % kev() == 0) CONAN_TRY(save_ckpt(i / kev()));
             double a = a_start[i], am = a + prm.da / 2;
             CONAN_TRY(pm.gkd(false, 0, true, pm.coef_drift(a, prm.da), true));
-            CONAN_TRY(pm.deposit());
-            CONAN_TRY(pm.poisson(am));
+            CONAN_TRY(pm.deposit_poisson(am));
             CONAN_TRY(pm.gkd(true, pm.coef_kick(am, prm.da), false, 0, false));
         }
         CONAN_TRY(pm.deposit());  // final density
@@ -440,8 +439,7 @@ template <typename T, int R> struct Diff : DiffBase {
             double a = a_start[i], am = a + prm.da / 2;
             double ck = pm.coef_kick(am, prm.da), cd = pm.coef_drift(a, prm.da);
             // forward force at d_{i+1}: deposit, potential, gradient mesh
-            CONAN_TRY(pm.deposit());
-            CONAN_TRY(pm.poisson(am));
+            CONAN_TRY(pm.deposit_poisson(am));
             // U = gather-transpose deposit of v = pbar
             const int nb = 296;
             k_absmax<T><<<nb, 256, 0, st>>>(pb[0], pb[1], pb[2], pm.np, R, part);

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "fft.cuh"
+#include "fft_plane.cuh"
 #include "fft_z.cuh"
 #include "ic.cuh"
 #include "pm.cuh"
@@ -202,6 +203,7 @@ template <typename T, int R> struct PM : PMBase {
             CONAN_TRY(zpass_setup());
             wbytes = std::max(wbytes, fft2.work_bytes);
             zpass = true;
+            if (lacc) CONAN_TRY(plane_setup());
         }
         CONAN_TRY(alloc((char **)&work, wbytes));
         CONAN_TRY(fft.bind(work, st));
@@ -456,13 +458,20 @@ template <typename T, int R> struct PM : PMBase {
         return drop_lag_deposit();
     }
 
-    int deposit_lag() {
+    // The Lagrangian deposit of the current positions into the accumulator
+    // mesh (unless the fused gather kernel did it already).
+    int lag_accumulate() {
         if (!lag_ready) {
             if (lag_v == 0) CONAN_TRY(launch_lag<0>());
             else if (lag_v == 1) CONAN_TRY(launch_lag<1>());
             else CONAN_TRY(launch_lag<2>());
         }
         lag_ready = false;
+        return CONAN_OK;
+    }
+
+    int deposit_lag() {
+        CONAN_TRY(lag_accumulate());
         size_t nt = (mf.cells + 3) / 4;  // four cells per thread
         CONAN_TIMED(prof, "deposit_mesh", st,
                     (k_acc_mesh<T><<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(lacc, mesh, mf.cells, mass)));
@@ -630,9 +639,125 @@ template <typename T, int R> struct PM : PMBase {
         }
     }
 
+    // Plane transforms by thread-block clusters (fft_plane.cuh; FP32 3D,
+    // n = 256 or 512, Lagrangian deposit): the forward pass reads the
+    // accumulator mesh directly, so the step's density is never written.
+    // plane_use: the autotuner's choice between them and cuFFT's planes
+    // (cuFFT until it is tuned: measured faster at 512^3 so far).
+    bool plane = false, plane_use = false;
+    bool plane_on() const { return plane && plane_use && zpass && lag_on(); }
+    int plane_kc = 16;       // kx columns per CTA of the plane pass
+    unsigned plane_kcs = 0;  // the column counts that launch here (bit 0: 16, bit 1: 32)
+    int plane_setup() {
+        if constexpr (sizeof(T) == 4 && R == 3) {
+            // CONAN_PLANE_PASS: 0 never, 1 from the start (else the autotuner decides)
+            const char *pp = getenv("CONAN_PLANE_PASS");
+            if (pp && *pp == '0') return CONAN_OK;
+            // 16 columns per CTA (clusters of 16 CTAs at n = 512) by default,
+            // 32 when only those launch; the autotuner times both
+            if (mf.n == 512) {
+                CONAN_TRY((plane_setup_n<512, 32>()));
+                CONAN_TRY((plane_setup_n<512, 16>()));
+            }
+            if (mf.n == 256) {
+                CONAN_TRY((plane_setup_n<256, 32>()));
+                CONAN_TRY((plane_setup_n<256, 16>()));
+            }
+            const char *kc = getenv("CONAN_PLANE_COLUMNS");  // 32: start with the 32-column variant
+            if (kc && atoi(kc) == 32 && (plane_kcs & 2u)) plane_kc = 32;
+            plane_use = plane && pp && *pp == '1';
+        }
+        return CONAN_OK;
+    }
+    // On when both kernels launch in clusters of PlaneT::C CTAs on this GPU.
+    template <int N, int KC> int plane_setup_n() {
+        typedef PlaneT<N, KC> PT;
+        if constexpr (PT::OK) {
+            auto fk = k_plane_fwd<N, KC>;
+            auto ik = k_plane_inv<N, KC>;
+            if (!raise_dyn_smem(fk, PT::SMEM) || !raise_dyn_smem(ik, PT::SMEM)) return CONAN_OK;
+            if (PT::C > 8 && (cudaFuncSetAttribute(fk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+                              cudaFuncSetAttribute(ik, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
+                cudaGetLastError();
+                return CONAN_OK;
+            }
+            cudaLaunchConfig_t cfg = plane_cfg<N, KC>();
+            cudaLaunchAttribute at;
+            plane_cluster(cfg, at);
+            int nc = 0;
+            if (cudaOccupancyMaxActiveClusters(&nc, fk, &cfg) != cudaSuccess || nc < 1 ||
+                cudaOccupancyMaxActiveClusters(&nc, ik, &cfg) != cudaSuccess || nc < 1) {
+                cudaGetLastError();
+                return CONAN_OK;
+            }
+            plane = true;
+            plane_kc = KC;
+            plane_kcs |= KC == 16 ? 1u : 2u;
+        }
+        return CONAN_OK;
+    }
+    template <int N, int KC> cudaLaunchConfig_t plane_cfg() const {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)PlaneT<N, KC>::C, (unsigned)mf.n, (unsigned)mf.batch);
+        cfg.blockDim = dim3((unsigned)PlaneT<N, KC>::THREADS);
+        cfg.dynamicSmemBytes = PlaneT<N, KC>::SMEM;
+        cfg.stream = st;
+        return cfg;
+    }
+    static void plane_cluster(cudaLaunchConfig_t &cfg, cudaLaunchAttribute &at) {
+        at.id = cudaLaunchAttributeClusterDimension;
+        at.val.clusterDim.x = cfg.gridDim.x;
+        at.val.clusterDim.y = 1;
+        at.val.clusterDim.z = 1;
+        cfg.attrs = &at;
+        cfg.numAttrs = 1;
+    }
+    template <int N, int KC> int plane_run(double gs) {
+        if constexpr (sizeof(T) == 4 && PlaneT<N, KC>::OK) {
+            cudaLaunchConfig_t cfg = plane_cfg<N, KC>();
+            cudaLaunchAttribute at;
+            plane_cluster(cfg, at);
+            float2 *sp = reinterpret_cast<float2 *>(spec);
+            CONAN_TIMED(prof, "plane_r2c", st,
+                        CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_fwd<N, KC>, (const unsigned long long *)lacc, sp,
+                                                      mf, 0x1p-23 * mass, (const float2 *)ztw)));
+            CONAN_TIMED(prof, "deposit_clear", st,
+                        CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st)));
+            CONAN_TRY(green_z(gs));
+            CONAN_TIMED(prof, "plane_c2r", st,
+                        CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_inv<N, KC>, (const float2 *)sp, (float *)mesh, mf,
+                                                      (const float2 *)ztw)));
+            return CONAN_OK;
+        } else {
+            return set_error(CONAN_ERR_UNSUPPORTED, "no plane pass for this mesh");
+        }
+    }
+
+    // The deposit of the current positions and the Poisson solve of the
+    // kick that follows it: through the cluster plane pass when it is on,
+    // else deposit() (density mesh) and poisson().
+    int deposit_poisson(double a) {
+        if (plane_on()) {
+            CONAN_TRY(lag_accumulate());
+            const double gs = poisson_scale(a);
+            if (mf.n == 512) CONAN_TRY((plane_kc == 16 ? plane_run<512, 16>(gs) : plane_run<512, 32>(gs)));
+            else CONAN_TRY((plane_kc == 16 ? plane_run<256, 16>(gs) : plane_run<256, 32>(gs)));
+            CONAN_TRY(fd_gradient(mesh, grad));
+            mesh_holds = 2;
+            return CONAN_OK;
+        }
+        CONAN_TRY(deposit());
+        return poisson(a);
+    }
+
+    // Green's function factor of a kick at a, with the per-member
+    // normalisation 1 / (cells of one box).
+    double poisson_scale(double a) const {
+        return -G / (a * (double)((size_t)1 << mf.cshift)) * std::pow(prm.size / (2 * M_PI), 2);
+    }
+
     int poisson(double a) {
-        // per-member normalisation: 1 / (cells of one box)
-        double gs = -G / (a * (double)((size_t)1 << mf.cshift)) * std::pow(prm.size / (2 * M_PI), 2);
+        const double gs = poisson_scale(a);
         if (zpass) {
             // 2D R2C of every z plane, z pass with the Green multiply, 2D C2R
             if constexpr (sizeof(T) == 4) {
@@ -852,6 +977,29 @@ template <typename T, int R> struct PM : PMBase {
             ztx = w[best];
             tuned[tuned.size() - w.size() + best].chosen = true;
         }
+        // (4) the x and y transforms of the planes: thread-block clusters or
+        // cuFFT's 2D plans
+        if (plane && lag_on()) {
+            struct PC { bool use; int kc; std::string name; };
+            std::vector<PC> pc = {{false, plane_kc, "cuFFT 2D plans"}};
+            for (int kc : {16, 32})
+                if (plane_kcs & (kc == 16 ? 1u : 2u))
+                    pc.push_back({true, kc, "thread-block clusters of " + std::to_string(mf.n / (2 * kc)) + " CTAs, " +
+                                                std::to_string(kc) + " columns each"});
+            best = -1;
+            bms = 1e30;
+            for (size_t i = 0; i < pc.size(); ++i) {
+                plane_use = pc[i].use;
+                plane_kc = pc[i].kc;
+                double ms = 0;
+                CONAN_TRY(tune_time(save, a, da, &ms));
+                tuned.push_back({"plane transforms", pc[i].name, ms, false});
+                if (ms < bms) bms = ms, best = (int)i;
+            }
+            plane_use = pc[best].use;
+            plane_kc = pc[best].kc;
+            tuned[tuned.size() - pc.size() + best].chosen = true;
+        }
         return CONAN_OK;
     }
 
@@ -949,8 +1097,7 @@ template <typename T, int R> struct PM : PMBase {
     }
 
     int kick(double a, double da) override {
-        CONAN_TRY(deposit());
-        CONAN_TRY(poisson(a));
+        CONAN_TRY(deposit_poisson(a));
         CONAN_TRY(gkd(true, coef_kick(a, da), false, 0, false));
         a_mom = a;
         return CONAN_OK;
@@ -963,8 +1110,7 @@ template <typename T, int R> struct PM : PMBase {
         a_pos = a;
         for (unsigned i = i0; i < i1; ++i) {
             double am = a + da / 2;
-            CONAN_TRY(deposit());
-            CONAN_TRY(poisson(am));
+            CONAN_TRY(deposit_poisson(am));
             bool last = i + 1 == i1;
             double an = a + da;
             CONAN_TRY(gkd(true, coef_kick(am, da), !last, last ? 0 : coef_drift(an, da), !last));
