@@ -177,11 +177,12 @@ template <int N, int KC, bool INV> __device__ inline void y_fft(float2 *Y, const
 
 // Grid (C, n, members), clusters of C CTAs along x: cluster (z, member)
 // transforms plane z. acc: the integer deposit (2^-23 units), kscale = 2^-23 x
-// particle mass; spec: the half spectra (z, ky, kx) of every plane.
+// particle mass; spec: the half spectra (z, ky, kx) of every plane; clear:
+// zero the accumulator behind the reads (instead of a memset after).
 template <int N, int KC>
 __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
-    k_plane_fwd(const unsigned long long *__restrict__ acc, float2 *__restrict__ spec, Mesh m, double kscale,
-                const float2 *__restrict__ twid) {
+    k_plane_fwd(unsigned long long *__restrict__ acc, float2 *__restrict__ spec, Mesh m, double kscale,
+                const float2 *__restrict__ twid, int clear) {
     typedef PlaneT<N, KC> P;
     constexpr int M = P::M, EPL = P::EPL;
     namespace cg = cooperative_groups;
@@ -200,10 +201,10 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
     // complex point l + 32 j of a row = its real points 2(l + 32 j), +1
     for (int i = warp; i < P::RY; i += P::WARPS) {
         const int y = P::RY * r + i;
-        const ulonglong2 *row = reinterpret_cast<const ulonglong2 *>(acc + mc + ((size_t)z * N + y) * N);
+        ulonglong2 *row = reinterpret_cast<ulonglong2 *>(acc + mc + ((size_t)z * N + y) * N);
         ulonglong2 a[EPL];
 #pragma unroll
-        for (int j = 0; j < EPL; ++j) a[j] = row[lane + 32 * j];
+        for (int j = 0; j < EPL; ++j) a[j] = __ldcs(row + lane + 32 * j);
         float2 v[EPL];
 #pragma unroll
         for (int j = 0; j < EPL; ++j)
@@ -225,6 +226,10 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
                 X = make_float2(e.x + t.x, e.y + t.y);
             }
             cl.map_shared_rank(Y, k / KC)[y * KC + k % KC] = X;
+        }
+        if (clear) {  // the accumulator is read once: leave the row cleared for the next deposit
+#pragma unroll
+            for (int j = 0; j < EPL; ++j) __stcs(row + lane + 32 * j, make_ulonglong2(0ull, 0ull));
         }
         __syncwarp();  // the scratch line is read before the next row overwrites it
     }
@@ -283,19 +288,24 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
     y_fft<N, KC, true>(Y, tw);
     cl.sync();  // every CTA's columns are transformed
     const size_t mc = (size_t)blockIdx.z << m.cshift;
-    for (int i = warp; i < P::RY; i += P::WARPS) {
-        const int y = P::RY * r + i;
-        // the row's X[k], k = l + 32 j, from column k % KC of CTA k / KC;
-        // X[0] and X[M] are the real and imaginary parts of the packed column
-        float2 x[EPL];
+    // the row's X[k], k = l + 32 j, from column k % KC of CTA k / KC (X[0]
+    // and X[M] are the real and imaginary parts of the packed column); the
+    // next row's values are fetched while this row is transformed
+    auto fetch = [&](int y, float2 (&x)[EPL]) {
 #pragma unroll
         for (int j = 0; j < EPL; ++j) {
             const int k = lane + 32 * j;
             x[j] = cl.map_shared_rank(Y, k / KC)[y * KC + k % KC];
         }
+    };
+    float2 x[EPL];
+    fetch(P::RY * r + warp, x);
+    for (int i = warp; i < P::RY; i += P::WARPS) {
+        const int y = P::RY * r + i;
 #pragma unroll
         for (int j = 0; j < EPL; ++j) s[spad(lane + 32 * j)] = x[j];
         __syncwarp();
+        if (i + P::WARPS < P::RY) fetch(y + P::WARPS, x);
         // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k])
         float2 v[EPL];
 #pragma unroll

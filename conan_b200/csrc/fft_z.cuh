@@ -177,6 +177,43 @@ __device__ inline void zstage(const ZIO &io, int Ns, const float2 *tw, const ZGr
     if constexpr (!OUT_G) __syncthreads();
 }
 
+// The forward transform's last stage (radix 8, sub-length N/8), the Green
+// multiply and the inverse transform's first stage (radix 8, sub-length 1)
+// in registers: thread j's eight outputs x[j + r N/8] of the one are the
+// eight inputs of the other, so the two stages share one shared-memory
+// round trip.
+template <int N, int TXW>
+__device__ inline void zstage_mid(const ZIO &io, const float2 *tw, const ZGreen &gf) {
+    constexpr int TX = ZTile<N, TXW>::TX, LT = ZTile<N, TXW>::LT;
+    static_assert(LT == N / 8, "one radix-8 butterfly per thread");
+    const int l = (int)threadIdx.x % TX, j = (int)threadIdx.x / TX;
+    float2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = io.buf[(j + r * LT) * TX + l];
+    __syncthreads();
+    // forward: twiddles exp(-2 pi i j r / N), then the radix-8 DFT
+    const float2 w1 = tw[j];
+    float2 wr = w1;
+#pragma unroll
+    for (int r = 1; r < 8; ++r) {
+        v[r] = cmul(v[r], wr);
+        wr = cmul(wr, w1);
+    }
+    dft_small<8, false>(v);
+    // natural-order index j + r N/8: the Green's function, then the inverse
+    // first stage (all twiddles 1) writing x[8 j + r]
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const float g = gf(j + r * LT, l);
+        v[r].x *= g;
+        v[r].y *= g;
+    }
+    dft_small<8, true>(v);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) io.buf[(8 * j + r) * TX + l] = v[r];
+    __syncthreads();
+}
+
 // Radix of stage s of an n-point transform: 8 while 8 divides the rest.
 template <int N> struct ZRadix {
     static constexpr int S8 = N >= 512 ? 3 : 2;  // radix-8 stages (64..1024 points)
@@ -204,17 +241,24 @@ __global__ void __launch_bounds__(ZTile<N, TXW>::THREADS, ZPASS_MIN_BLOCKS) k_zp
     const int wy = wave_index(ky, m.n);
     const ZGreen gf{(long long)wy * wy, kx0, m.n, gs};
     constexpr int S8 = ZRadix<N>::S8, REST = ZRadix<N>::REST;
-    // forward: radix-8 stages (the first from global memory), then the rest
+    // forward: the radix-2/4 stage first (from global memory) when n is not
+    // a power of 8, then the radix-8 stages, the last of them fused with the
+    // Green multiply and the inverse's first stage (zstage_mid); the inverse
+    // goes on with radix 8 and ends with the radix-2/4 stage (to global)
     int Ns = 1;
-    zstage<N, TXW, 8, false, true, false, false>(io, Ns, tw, gf);
-    Ns *= 8;
+    if constexpr (REST > 1) {
+        zstage<N, TXW, REST, false, true, false, false>(io, Ns, tw, gf);
+        Ns *= REST;
+        zstage<N, TXW, 8, false, false, false, false>(io, Ns, tw, gf);
+        Ns *= 8;
+    } else {
+        zstage<N, TXW, 8, false, true, false, false>(io, Ns, tw, gf);
+        Ns *= 8;
+    }
 #pragma unroll
-    for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, TXW, 8, false, false, false, false>(io, Ns, tw, gf);
-    if constexpr (REST > 1) zstage<N, TXW, REST, false, false, false, false>(io, Ns, tw, gf);
-    // inverse, the Green's function applied as the first stage reads
-    Ns = 1;
-    zstage<N, TXW, 8, true, false, false, true>(io, Ns, tw, gf);
-    Ns *= 8;
+    for (int s = 2; s < S8; ++s, Ns *= 8) zstage<N, TXW, 8, false, false, false, false>(io, Ns, tw, gf);
+    zstage_mid<N, TXW>(io, tw, gf);
+    Ns = 8;
     if constexpr (REST > 1) {
 #pragma unroll
         for (int s = 1; s < S8; ++s, Ns *= 8) zstage<N, TXW, 8, true, false, false, false>(io, Ns, tw, gf);

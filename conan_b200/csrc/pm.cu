@@ -8,6 +8,11 @@
 
 #include "fft.cuh"
 #include "fft_plane.cuh"
+// The forward plane pass zeroes the accumulator behind its reads (1) or a
+// memset does it afterwards (0); a compile-time tunable.
+#ifndef PLANE_CLEAR
+#define PLANE_CLEAR 1
+#endif
 #include "fft_z.cuh"
 #include "ic.cuh"
 #include "pm.cuh"
@@ -642,15 +647,18 @@ template <typename T, int R> struct PM : PMBase {
     // Plane transforms by thread-block clusters (fft_plane.cuh; FP32 3D,
     // n = 256 or 512, Lagrangian deposit): the forward pass reads the
     // accumulator mesh directly, so the step's density is never written.
-    // plane_use: the autotuner's choice between them and cuFFT's planes
-    // (cuFFT until it is tuned: measured faster at 512^3 so far).
+    // plane_use: the autotuner's choice between them and cuFFT's planes.
     bool plane = false, plane_use = false;
+    bool plane_inv = true;  // the inverse too (else cuFFT's 2D C2R after the z pass)
+    bool plane_clear = PLANE_CLEAR;  // the forward pass clears the accumulator (else a memset)
     bool plane_on() const { return plane && plane_use && zpass && lag_on(); }
     int plane_kc = 16;       // kx columns per CTA of the plane pass
     unsigned plane_kcs = 0;  // the column counts that launch here (bit 0: 16, bit 1: 32)
     int plane_setup() {
         if constexpr (sizeof(T) == 4 && R == 3) {
-            // CONAN_PLANE_PASS: 0 never, 1 from the start (else the autotuner decides)
+            // CONAN_PLANE_PASS: 0 never, 1 both passes from the start, 2 the
+            // forward pass from the start (else the default below, until the
+            // autotuner decides)
             const char *pp = getenv("CONAN_PLANE_PASS");
             if (pp && *pp == '0') return CONAN_OK;
             // 16 columns per CTA (clusters of 16 CTAs at n = 512) by default,
@@ -663,9 +671,22 @@ template <typename T, int R> struct PM : PMBase {
                 CONAN_TRY((plane_setup_n<256, 32>()));
                 CONAN_TRY((plane_setup_n<256, 16>()));
             }
-            const char *kc = getenv("CONAN_PLANE_COLUMNS");  // 32: start with the 32-column variant
+            if (!plane) return CONAN_OK;
+            // 32 columns per CTA: at 512^3 0.67 ms per forward pass against 0.69
+            // with 16 (and 0.70 against 0.81 per inverse pass)
+            if (plane_kcs & 2u) plane_kc = 32;
+            const char *kc = getenv("CONAN_PLANE_COLUMNS");
+            if (kc && atoi(kc) == 16 && (plane_kcs & 1u)) plane_kc = 16;
             if (kc && atoi(kc) == 32 && (plane_kcs & 2u)) plane_kc = 32;
-            plane_use = plane && pp && *pp == '1';
+            if (pp && (*pp == '1' || *pp == '2')) {
+                plane_use = true;
+                plane_inv = *pp == '1';  // 2: the forward pass only
+            } else {
+                // measured at 512^3: the forward pass here, cuFFT's inverse
+                // (5.86 against 5.96 ms per step); elsewhere the autotuner decides
+                plane_use = mf.n == 512;
+                plane_inv = false;
+            }
         }
         return CONAN_OK;
     }
@@ -719,14 +740,18 @@ template <typename T, int R> struct PM : PMBase {
             plane_cluster(cfg, at);
             float2 *sp = reinterpret_cast<float2 *>(spec);
             CONAN_TIMED(prof, "plane_r2c", st,
-                        CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_fwd<N, KC>, (const unsigned long long *)lacc, sp,
-                                                      mf, 0x1p-23 * mass, (const float2 *)ztw)));
-            CONAN_TIMED(prof, "deposit_clear", st,
-                        CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st)));
+                        CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_fwd<N, KC>, lacc, sp, mf, 0x1p-23 * mass,
+                                                      (const float2 *)ztw, plane_clear ? 1 : 0)));
+            if (!plane_clear)
+                CONAN_TIMED(prof, "deposit_clear", st,
+                            CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st)));
             CONAN_TRY(green_z(gs));
-            CONAN_TIMED(prof, "plane_c2r", st,
-                        CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_inv<N, KC>, (const float2 *)sp, (float *)mesh, mf,
-                                                      (const float2 *)ztw)));
+            if (plane_inv)
+                CONAN_TIMED(prof, "plane_c2r", st,
+                            CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_inv<N, KC>, (const float2 *)sp, (float *)mesh,
+                                                          mf, (const float2 *)ztw)));
+            else
+                CONAN_TIMED(prof, "fft_c2r", st, CONAN_TRY(fft2.inverse(spec, mesh)));
             return CONAN_OK;
         } else {
             return set_error(CONAN_ERR_UNSUPPORTED, "no plane pass for this mesh");
@@ -980,16 +1005,20 @@ template <typename T, int R> struct PM : PMBase {
         // (4) the x and y transforms of the planes: thread-block clusters or
         // cuFFT's 2D plans
         if (plane && lag_on()) {
-            struct PC { bool use; int kc; std::string name; };
-            std::vector<PC> pc = {{false, plane_kc, "cuFFT 2D plans"}};
+            struct PC { bool use, inv; int kc; std::string name; };
+            std::vector<PC> pc = {{false, true, plane_kc, "cuFFT 2D plans"}};
             for (int kc : {16, 32})
-                if (plane_kcs & (kc == 16 ? 1u : 2u))
-                    pc.push_back({true, kc, "thread-block clusters of " + std::to_string(mf.n / (2 * kc)) + " CTAs, " +
-                                                std::to_string(kc) + " columns each"});
+                if (plane_kcs & (kc == 16 ? 1u : 2u)) {
+                    const std::string cl = "thread-block clusters of " + std::to_string(mf.n / (2 * kc)) + " CTAs, " +
+                                           std::to_string(kc) + " columns each";
+                    pc.push_back({true, true, kc, cl});
+                    pc.push_back({true, false, kc, cl + " (forward; cuFFT inverse)"});
+                }
             best = -1;
             bms = 1e30;
             for (size_t i = 0; i < pc.size(); ++i) {
                 plane_use = pc[i].use;
+                plane_inv = pc[i].inv;
                 plane_kc = pc[i].kc;
                 double ms = 0;
                 CONAN_TRY(tune_time(save, a, da, &ms));
@@ -997,6 +1026,7 @@ template <typename T, int R> struct PM : PMBase {
                 if (ms < bms) bms = ms, best = (int)i;
             }
             plane_use = pc[best].use;
+            plane_inv = pc[best].inv;
             plane_kc = pc[best].kc;
             tuned[tuned.size() - pc.size() + best].chosen = true;
         }

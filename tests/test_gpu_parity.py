@@ -295,8 +295,9 @@ def test_plane_transforms_and_z_pass_give_the_3d_potential(gpu, conan, Nm, f):
     assert rel(phis["fp32"], phis["fp64"]) < 2e-5
 
 
-@pytest.mark.parametrize("Nm,f,columns", [(256, 1, 16), (64, 8, 16), (128, 2, 16), (64, 8, 32), (128, 2, 32)])
-def test_cluster_plane_pass_matches_cufft_planes(gpu, conan, monkeypatch, Nm, f, columns):
+@pytest.mark.parametrize("Nm,f,columns,mode", [(256, 1, 16, "1"), (64, 8, 16, "1"), (128, 2, 16, "1"),
+                                               (64, 8, 32, "1"), (128, 2, 32, "1"), (64, 8, 32, "2")])
+def test_cluster_plane_pass_matches_cufft_planes(gpu, conan, monkeypatch, Nm, f, columns, mode):
     """256^3 and 512^3 FP32 meshes transform their z planes in thread-block
     clusters (the forward pass reading the integer deposit directly); the
     potential and the kicked momenta equal those of cuFFT's plane transforms
@@ -305,15 +306,15 @@ def test_cluster_plane_pass_matches_cufft_planes(gpu, conan, monkeypatch, Nm, f,
     X, Pm = _particles(3, Nm, f, L, 2.0, 9)
     out = {}
     monkeypatch.setenv("CONAN_PLANE_COLUMNS", str(columns))
-    for on in ("0", "1"):
+    for on in ("0", mode):  # mode 2: the cluster forward pass, cuFFT's inverse
         monkeypatch.setenv("CONAN_PLANE_PASS", on)
         g = conan.Gravity(3, Nm, f, L, precision="fp32")
         g.set_state(X, Pm, 0.4, 0.4)
         g.set_profiling(True)
         g.kick(0.4, 0.01)
         kernels = set(g.profile())
-        assert ("plane_r2c" in kernels and "plane_c2r" in kernels) == (on == "1"), kernels
+        assert ("plane_r2c" in kernels) == (on != "0") and ("plane_c2r" in kernels) == (on == "1"), kernels
         out[on] = (g.potential(), g.state()[1])
         g.close()
-    assert rel(out["1"][0], out["0"][0]) < 2e-6
-    assert rel(out["1"][1], out["0"][1]) < 2e-6
+    assert rel(out[mode][0], out["0"][0]) < 2e-6
+    assert rel(out[mode][1], out["0"][1]) < 2e-6
