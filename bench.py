@@ -595,12 +595,20 @@ def run_ours(args):
                                   "deposit_mesh", "deposit_clear"), dep_b + gat_b),) if fused else
              (("deposit", ("rank", "scan", "scatter", "deposit", "deposit_mesh", "deposit_clear"), dep_b),
               ("gather", ("fd_grad", "gather_kick_drift", "gather_kick", "drift"), gat_b)))
+    # with the cluster plane pass the accumulator goes straight into the
+    # forward transform: no density is written, so the row does not count it
+    folded = "plane_r2c" in prof
     for row, ks, ab_row in table:
         t = sum(prof[k][1] for k in ks if k in prof) / args.steps
+        if folded and row in ("gather+deposit", "deposit"):
+            ab_row -= 4 * Nc
         if t > 0:
             rows[row] = {"kernels": [k for k in ks if k in prof], "ms_per_step": t,
                          "algorithmic_bytes": ab_row, "achieved": ab_row / (t * 1e-3) / 1e9,
                          "frac": ab_row / (t * 1e-3) / 1e9 / hbm}
+            if folded and row in ("gather+deposit", "deposit"):
+                rows[row]["density"] = "converted and cleared inside plane_r2c (the forward plane transform)"
+
     roof["rows"] = rows
     step_bytes = 60 * Np + 24 * Nc
     kernels = {k: {"launches": v[0], "ms_total": round(v[1], 4), "share": round(v[1] / max(1e-9, sum(

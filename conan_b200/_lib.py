@@ -110,6 +110,7 @@ SIGNATURES = {
     "conan_ens_forward_adjoint": (C.c_int, [C.c_void_p, _dp]),
     "conan_ens_power_spectrum": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp]),
     "conan_ens_state": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
+    "conan_ens_member_fields": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _dp]),
     "conan_ens_last_ms": (C.c_int, [C.c_void_p, _dp, _dp]),
     "conan_ens_total_particles": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "conan_ens_describe": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),

@@ -38,6 +38,7 @@ struct EnsBase {
     virtual int forward_adjoint(double *loss) = 0;
     virtual int power_spectrum(int member, int nbins, double *k, double *P, double *cnt) = 0;
     virtual int state(int member, double *X, double *P) = 0;
+    virtual int member_fields(int member, double *noise, double *target, double *gnoise) = 0;
     virtual int last_ms(double *run_ms, double *adj_ms) = 0;
     virtual size_t total_particles() const = 0;
     virtual std::string describe() const = 0;
@@ -64,6 +65,7 @@ template <typename T, int R> struct Ens : EnsBase {
     cudaGraphExec_t graph = nullptr;
     double run_ms = 0, adj_ms = 0;
     bool ready = false;
+    bool have_grad = false;  // the noise gradients of a forward_adjoint are in gn
 
     ~Ens() override {
         if (main) cudaStreamSynchronize(main);
@@ -296,6 +298,7 @@ template <typename T, int R> struct Ens : EnsBase {
             CONAN_TRY(c.d->pm.check_err());
         }
         adj_ms = total;
+        have_grad = true;
         return CONAN_OK;
     }
 
@@ -323,6 +326,25 @@ template <typename T, int R> struct Ens : EnsBase {
         }
         v.np = np1;
         return pm.export_state(v, np1, X, Pm);
+    }
+
+    int member_fields(int member, double *noise, double *target, double *gnoise) override {
+        if (member < 0 || member >= (int)mem.size()) return set_error(CONAN_ERR_ARG, "no member %d", member);
+        if (!ready) return set_error(CONAN_ERR_STATE, "call conan_ens_init first");
+        if (gnoise && !have_grad) return set_error(CONAN_ERR_STATE, "no gradient: call conan_ens_forward_adjoint first");
+        auto &c = cls[where[member].first];
+        auto &pm = c.d->pm;
+        const size_t n1 = (size_t)1 << pm.mf.cshift, o = (size_t)where[member].second * n1;
+        std::vector<T> h(n1);
+        const T *src[3] = {c.noise + o, c.target + o, c.gn + o};
+        double *dst[3] = {noise, target, gnoise};
+        CONAN_CUDA(cudaStreamSynchronize(pm.st));
+        for (int f = 0; f < 3; ++f) {
+            if (!dst[f]) continue;
+            CONAN_CUDA(cudaMemcpy(h.data(), src[f], n1 * sizeof(T), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n1; ++i) dst[f][i] = (double)h[i];
+        }
+        return CONAN_OK;
     }
 
     int last_ms(double *r, double *a) override {

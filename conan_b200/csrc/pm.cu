@@ -1699,6 +1699,10 @@ int conan_ens_state(conan_ens *h, int member, double *X, double *P) {
     ENS_GUARD(h);
     return h->impl->state(member, X, P);
 }
+int conan_ens_member_fields(conan_ens *h, int member, double *noise, double *target, double *gnoise) {
+    ENS_GUARD(h);
+    return h->impl->member_fields(member, noise, target, gnoise);
+}
 int conan_ens_last_ms(conan_ens *h, double *run_ms, double *adjoint_ms) {
     ENS_GUARD(h);
     return h->impl->last_ms(run_ms, adjoint_ms);

@@ -120,6 +120,16 @@ class Ensemble:
         L.check(L.lib().conan_ens_state(self._h, member, L.ptr(X), L.ptr(P)))
         return X, P
 
+    def member_fields(self, member: int, gradient: bool = True):
+        """(white noise, target density, d loss / d noise) of a member; the
+        gradient is that of the last forward_adjoint (None if gradient=False)."""
+        n = (1 << self.members[member][0]) ** self.dim
+        noise, target = np.empty(n), np.empty(n)
+        g = np.empty(n) if gradient else None
+        L.check(L.lib().conan_ens_member_fields(self._h, member, L.ptr(noise), L.ptr(target),
+                                                L.ptr(g) if gradient else None))
+        return noise, target, g
+
     def mean_power_spectrum(self, nbins: int, dist=None):
         """Mean P(k) over the members (and ranks), bins of width 2 pi / L."""
         Ps, cnt = [], np.zeros(nbins)

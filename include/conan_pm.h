@@ -307,8 +307,8 @@ int conan_diff_backward(conan_diff *h, const void *grad_density_dev, void *grad_
 /* -------------------------------------------------------- ensemble -- */
 
 /* A batch of independent realisations with possibly different mesh sizes,
- * run together: every phase of a step is one persistent launch over all
- * members, and the whole run is one CUDA graph. */
+ * run together: every phase of a step is one launch over all members of a
+ * size class, and the whole run is one CUDA graph. */
 typedef struct {
     int mbits;           /* N = 1 << mbits particles and mesh cells per side */
     double size;         /* L */
@@ -342,6 +342,12 @@ int conan_ens_forward_adjoint(conan_ens *h, double *loss_out);
 int conan_ens_power_spectrum(conan_ens *h, int member, int nbins, double *k, double *P,
                              double *count);
 int conan_ens_state(conan_ens *h, int member, double *X, double *P);
+/* A member's white noise, its target density (the model run from seed +
+ * 1000000) and, after conan_ens_forward_adjoint, the gradient of its loss
+ * with respect to the noise: host doubles, N^dim values each; a null
+ * pointer skips that field. No reference counterpart (for checking the
+ * batched adjoint against a single-box one). */
+int conan_ens_member_fields(conan_ens *h, int member, double *noise, double *target, double *gnoise);
 /* Milliseconds of the last conan_ens_run / forward_adjoint (CUDA events). */
 int conan_ens_last_ms(conan_ens *h, double *run_ms, double *adjoint_ms);
 int conan_ens_total_particles(conan_ens *h, size_t *n);

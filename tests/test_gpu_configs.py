@@ -138,6 +138,36 @@ def test_ensemble_32_class_against_the_oracle(gpu, conan, oracle):
     assert mean_err < 1e-3 and per.max() < 1e-3
 
 
+def test_ensemble_gradient_against_the_cpu_adjoint(gpu, conan, oracle):
+    """The batched forward + adjoint of the ensemble (two 32^3 members of
+    the 96-box set, L = 100, 40 steps a = 0.05 -> 1, FP32, checkpoint 8):
+    each member's loss (mean squared difference to its target density) and
+    its gradient with respect to the white noise against the FP64 CPU model
+    and adjoint run on the same noise and target."""
+    from conan_b200.ensemble import Ensemble, standard_members
+    members = standard_members()[:2]
+    steps = 40
+    e = Ensemble(members, precision="fp32", steps=steps)
+    e.init()
+    loss = e.forward_adjoint()
+    fields = [e.member_fields(i) for i in range(len(members))]
+    e.close()
+    for i, (mb, L, ns, seed) in enumerate(members):
+        noise, target, g = fields[i]
+        args = (3, mb, 1, L, ns, False, 8.0, 0.83, 0.05, 0.95 / steps, steps, noise)
+        dref = oracle.diff_forward(*args)
+        lref = float(np.mean((dref - target) ** 2))
+        _, gref = oracle.diff_adjoint(*args, 2 * (dref - target) / dref.size)
+        scale = np.max(np.abs(gref))
+        rel_max = float(np.max(np.abs(g - gref)) / scale)
+        big = np.abs(gref) > 1e-2 * scale
+        rel = np.abs(g - gref)[big] / np.abs(gref)[big]
+        lerr = abs(loss[i] - lref) / lref
+        print(f"ensemble member {i} (32^3, 40 steps) FP32 vs FP64 CPU adjoint: loss rel err {lerr:.2e}; "
+              f"max |dg| / max |g| {rel_max:.2e}; median rel (components above 1%) {np.median(rel):.2e}")
+        assert lerr < 1e-4 and rel_max < 5e-3 and np.median(rel) < 1e-3
+
+
 def test_ensemble_mean_pk_fp32_against_fp64(gpu, conan):
     from conan_b200.ensemble import Ensemble, standard_members
     members = standard_members(n_per_class=4)
