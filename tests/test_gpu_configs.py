@@ -165,7 +165,8 @@ def test_ensemble_gradient_against_the_cpu_adjoint(gpu, conan, oracle):
         lerr = abs(loss[i] - lref) / lref
         print(f"ensemble member {i} (32^3, 40 steps) FP32 vs FP64 CPU adjoint: loss rel err {lerr:.2e}; "
               f"max |dg| / max |g| {rel_max:.2e}; median rel (components above 1%) {np.median(rel):.2e}")
-        assert lerr < 1e-4 and rel_max < 5e-3 and np.median(rel) < 1e-3
+        # measured on a B200: loss 1.3e-6, max 1.1e-4 of the largest component, median 3.7e-5
+        assert lerr < 1e-5 and rel_max < 1e-3 and np.median(rel) < 2e-4
 
 
 def test_ensemble_mean_pk_fp32_against_fp64(gpu, conan):
