@@ -198,17 +198,37 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
     // row lands in another CTA's columns
     __syncthreads();
     cluster_arrive_wait_relaxed();
-    // complex point l + 32 j of a row = its real points 2(l + 32 j), +1
+    // complex point l + 32 j of a row = its real points 2(l + 32 j), +1; with
+    // the register budget of one CTA per SM, the next row's loads are issued
+    // before this row's transform
+    constexpr bool PREFETCH = P::MINB == 1;
+    auto row_of = [&](int i) { return reinterpret_cast<ulonglong2 *>(acc + mc + ((size_t)z * N + P::RY * r + i) * N); };
+    ulonglong2 a[EPL];
+    float2 *dst[PREFETCH ? EPL : 1];  // the owners' columns of this lane's kx (same for every row)
+    if constexpr (PREFETCH) {
+#pragma unroll
+        for (int j = 0; j < EPL; ++j) {
+            a[j] = __ldcs(row_of(warp) + lane + 32 * j);
+            dst[j] = cl.map_shared_rank(Y, (lane + 32 * j) / KC);
+        }
+    }
     for (int i = warp; i < P::RY; i += P::WARPS) {
         const int y = P::RY * r + i;
-        ulonglong2 *row = reinterpret_cast<ulonglong2 *>(acc + mc + ((size_t)z * N + y) * N);
-        ulonglong2 a[EPL];
+        ulonglong2 *row = row_of(i);
+        if constexpr (!PREFETCH) {
 #pragma unroll
-        for (int j = 0; j < EPL; ++j) a[j] = __ldcs(row + lane + 32 * j);
+            for (int j = 0; j < EPL; ++j) a[j] = __ldcs(row + lane + 32 * j);
+        }
         float2 v[EPL];
 #pragma unroll
         for (int j = 0; j < EPL; ++j)
             v[j] = make_float2((float)((double)a[j].x * kscale - 1.0), (float)((double)a[j].y * kscale - 1.0));
+        if constexpr (PREFETCH) {
+            if (i + P::WARPS < P::RY) {
+#pragma unroll
+                for (int j = 0; j < EPL; ++j) a[j] = __ldcs(row_of(i + P::WARPS) + lane + 32 * j);
+            }
+        }
         warp_fft<N, false>(v, s, tw);
         // split: X[k] = (Z[k] + conj Z[M-k]) / 2 - i W^k (Z[k] - conj Z[M-k]) / 2;
         // kx = k goes to column k % KC of CTA k / KC
@@ -225,7 +245,8 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
                 const float2 t = cmul(tw[k], o);
                 X = make_float2(e.x + t.x, e.y + t.y);
             }
-            cl.map_shared_rank(Y, k / KC)[y * KC + k % KC] = X;
+            if constexpr (PREFETCH) dst[j][y * KC + k % KC] = X;
+            else cl.map_shared_rank(Y, k / KC)[y * KC + k % KC] = X;
         }
         if (clear) {  // the accumulator is read once: leave the row cleared for the next deposit
 #pragma unroll
@@ -267,7 +288,7 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
     for (int i = threadIdx.x; i < N; i += P::THREADS) tw[i] = twid[i];
     const int r = (int)cl.block_rank(), z = (int)blockIdx.y;
     const float2 *in = spec + (size_t)blockIdx.z * m.mspec + (size_t)z * N * m.nh;
-    constexpr int PER = N * KC / P::THREADS, BATCH = PER < 8 ? PER : 8;
+    constexpr int PER = N * KC / P::THREADS, BATCH = (P::MINB == 1 || PER < 8) ? PER : 8;
 #pragma unroll
     for (int q0 = 0; q0 < PER; q0 += BATCH) {
         float2 v0[BATCH];  // a batch of the column loads in flight at once
