@@ -616,9 +616,10 @@ __global__ void __launch_bounds__(512) k_fd_grad(const T *__restrict__ phi, G4<T
 // The same gradient for 3D meshes of at least 32 cells per side, marching
 // along z: a CTA of 32 x 8 threads takes a 32 x 8 column of cells over FZ
 // planes. Each plane's tile with a two-cell halo in x and y is staged in
-// shared memory (two buffers, one barrier per plane) for the x and y
-// differences, and each thread keeps its column's five z values in
-// registers; the same arithmetic as k_fd_grad, so the same bits.
+// shared memory (two buffers, one barrier per plane, the next plane's loads
+// in flight while a plane is computed) for the x and y differences, and
+// each thread keeps its column's five z values in registers; the same
+// arithmetic as k_fd_grad, so the same bits.
 #ifndef FD_GRAD_ZM
 #define FD_GRAD_ZM 0
 #endif
@@ -649,21 +650,47 @@ __global__ void __launch_bounds__(256) k_fd_grad_zm(const T *__restrict__ phi, G
     T q[5];  // this column at z - 2 .. z + 2
 #pragma unroll
     for (int j = 0; j < 5; ++j) q[j] = at(x0 + tx, y0 + ty, z0 - 2 + j);
+    // this thread's share of a plane's 12 x 36 halo tile (elements threadIdx,
+    // threadIdx + 256): the next plane's share is loaded while this plane is
+    // computed, and stored into the other buffer at the top of the next
+    // iteration (the barrier of this iteration orders it after every read of
+    // that buffer two planes back)
+    constexpr int TE = 12 * 36;
+    auto tile_at = [&](int e, int zz) {
+        const int r = e / 36, c = e - r * 36;
+        return at(x0 - 2 + c, y0 - 2 + r, zz);
+    };
+    T nxt[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int e = (int)threadIdx.x + 256 * k;
+        nxt[k] = e < TE ? tile_at(e, z0) : T(0);
+    }
     for (int zi = 0; zi < FDZ_PLANES; ++zi) {
         const int z = z0 + zi;
         T(*t)[36] = tile[zi & 1];
-        for (int e = threadIdx.x; e < 12 * 36; e += 256) {
-            const int r = e / 36, c = e - r * 36;
-            t[r][c] = at(x0 - 2 + c, y0 - 2 + r, z);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int e = (int)threadIdx.x + 256 * k;
+            if (e < TE) t[e / 36][e % 36] = nxt[k];
         }
         __syncthreads();
+        T q4n = T(0);
+        if (zi + 1 < FDZ_PLANES) {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int e = (int)threadIdx.x + 256 * k;
+                if (e < TE) nxt[k] = tile_at(e, z + 1);
+            }
+            q4n = at(x0 + tx, y0 + ty, z + 3);
+        }
         const T gx = (t[ty + 2][tx] - t[ty + 2][tx + 4]) * c12 + (t[ty + 2][tx + 3] - t[ty + 2][tx + 1]) * c23;
         const T gy = (t[ty][tx + 2] - t[ty + 4][tx + 2]) * c12 + (t[ty + 3][tx + 2] - t[ty + 1][tx + 2]) * c23;
         const T gz = (q[0] - q[4]) * c12 + (q[3] - q[1]) * c23;
         g[((size_t)z << (2 * s)) | ((size_t)(y0 + ty) << s) | (size_t)(x0 + tx)] = G4<T>{gx, gy, gz, T(0)};
 #pragma unroll
         for (int j = 0; j < 4; ++j) q[j] = q[j + 1];
-        if (zi + 1 < FDZ_PLANES) q[4] = at(x0 + tx, y0 + ty, z + 3);
+        q[4] = q4n;
     }
 }
 
