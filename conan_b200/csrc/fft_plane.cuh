@@ -202,7 +202,9 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
     // the register budget of one CTA per SM, the next row's loads are issued
     // before this row's transform
     constexpr bool PREFETCH = P::MINB == 1;
-    auto row_of = [&](int i) { return reinterpret_cast<ulonglong2 *>(acc + mc + ((size_t)z * N + P::RY * r + i) * N); };
+    auto row_of = [&](int i) {
+        return reinterpret_cast<ulonglong2 *>(acc + mc + ((size_t)z * N + P::RY * r + i) * N);
+    };
     ulonglong2 a[EPL];
     float2 *dst[PREFETCH ? EPL : 1];  // the owners' columns of this lane's kx (same for every row)
     if constexpr (PREFETCH) {
@@ -235,13 +237,13 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
 #pragma unroll
         for (int j = 0; j < EPL; ++j) {
             const int k = lane + 32 * j;
-            const float2 a = s[spad(k)], b = s[spad((M - k) & (M - 1))];
+            const float2 za = s[spad(k)], zb = s[spad((M - k) & (M - 1))];
             float2 X;
             if (k == 0) {
-                X = make_float2(a.x + a.y, a.x - a.y);  // DC + i Nyquist, both real
+                X = make_float2(za.x + za.y, za.x - za.y);  // DC + i Nyquist, both real
             } else {
-                const float2 e = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));  // (Z + conj Zc) / 2
-                const float2 o = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));  // (Z - conj Zc) / 2i
+                const float2 e = make_float2(0.5f * (za.x + zb.x), 0.5f * (za.y - zb.y));  // (Z + conj Zc) / 2
+                const float2 o = make_float2(0.5f * (za.y + zb.y), -0.5f * (za.x - zb.x));  // (Z - conj Zc) / 2i
                 const float2 t = cmul(tw[k], o);
                 X = make_float2(e.x + t.x, e.y + t.y);
             }

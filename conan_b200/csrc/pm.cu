@@ -661,8 +661,8 @@ template <typename T, int R> struct PM : PMBase {
             // autotuner decides)
             const char *pp = getenv("CONAN_PLANE_PASS");
             if (pp && *pp == '0') return CONAN_OK;
-            // 16 columns per CTA (clusters of 16 CTAs at n = 512) by default,
-            // 32 when only those launch; the autotuner times both
+            // both column counts (clusters of 8 and of 16 CTAs at n = 512)
+            // where they launch; the autotuner times both
             if (mf.n == 512) {
                 CONAN_TRY((plane_setup_n<512, 32>()));
                 CONAN_TRY((plane_setup_n<512, 16>()));
@@ -683,7 +683,7 @@ template <typename T, int R> struct PM : PMBase {
                 plane_inv = *pp == '1';  // 2: the forward pass only
             } else {
                 // measured at 512^3: the forward pass here, cuFFT's inverse
-                // (5.86 against 5.96 ms per step); elsewhere the autotuner decides
+                // (5.82 against 5.99 ms per step); elsewhere the autotuner decides
                 plane_use = mf.n == 512;
                 plane_inv = false;
             }
