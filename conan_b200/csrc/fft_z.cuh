@@ -27,13 +27,20 @@
 namespace conan {
 
 // Lines per CTA and threads per CTA for an n-point z transform: n / 8
-// threads per line. (At n = 1024, 4 lines per CTA instead of 8 measured
+// threads per line (n / 16 at 1024 points). (At n = 1024, 4 lines per CTA instead of 8 measured
 // slower: 31.0 against 30.0 ms per step of the 1024^3-mesh run.)
 // TX = 0 takes the default width; the autotuner also tries half and twice
 // the default (ZTile<N, TX>::OK says whether a width fits one CTA).
+// Threads per line at 1024 points: 128 (one radix-8 butterfly per thread
+// and stage, one 1024-thread CTA per SM) or 64 (two butterflies, two
+// 512-thread CTAs per SM: 4.27 against 4.85 ms per pass on the 1024^3
+// mesh); a compile-time tunable.
+#ifndef ZPASS_LT1024
+#define ZPASS_LT1024 64
+#endif
 template <int N, int TX_ = 0> struct ZTile {
     static constexpr int TX = TX_ ? TX_ : (N >= 256 ? 8 : 2048 / N);
-    static constexpr int LT = N / 8;  // threads per line
+    static constexpr int LT = N == 1024 ? ZPASS_LT1024 : N / 8;  // threads per line
     static constexpr int THREADS = TX * LT;
     static constexpr size_t SMEM = (size_t)TX * N * sizeof(float2) + (size_t)N * sizeof(float2);
     static constexpr bool OK = THREADS <= 1024 && SMEM <= 200 * 1024;
@@ -184,33 +191,39 @@ __device__ inline void zstage(const ZIO &io, int Ns, const float2 *tw, const ZGr
 // round trip.
 template <int N, int TXW>
 __device__ inline void zstage_mid(const ZIO &io, const float2 *tw, const ZGreen &gf) {
-    constexpr int TX = ZTile<N, TXW>::TX, LT = ZTile<N, TXW>::LT;
-    static_assert(LT == N / 8, "one radix-8 butterfly per thread");
-    const int l = (int)threadIdx.x % TX, j = (int)threadIdx.x / TX;
-    float2 v[8];
+    constexpr int TX = ZTile<N, TXW>::TX, LT = ZTile<N, TXW>::LT, NB = N / 8, Q = NB / LT;
+    static_assert(Q * LT == NB, "whole radix-8 butterflies per thread");
+    const int l = (int)threadIdx.x % TX, j0 = (int)threadIdx.x / TX;
+    float2 v[Q][8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = io.buf[(j + r * LT) * TX + l];
+    for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) v[q][r] = io.buf[(j0 + q * LT + r * NB) * TX + l];
     __syncthreads();
-    // forward: twiddles exp(-2 pi i j r / N), then the radix-8 DFT
-    const float2 w1 = tw[j];
-    float2 wr = w1;
 #pragma unroll
-    for (int r = 1; r < 8; ++r) {
-        v[r] = cmul(v[r], wr);
-        wr = cmul(wr, w1);
+    for (int q = 0; q < Q; ++q) {
+        const int j = j0 + q * LT;
+        // forward: twiddles exp(-2 pi i j r / N), then the radix-8 DFT
+        const float2 w1 = tw[j];
+        float2 wr = w1;
+#pragma unroll
+        for (int r = 1; r < 8; ++r) {
+            v[q][r] = cmul(v[q][r], wr);
+            wr = cmul(wr, w1);
+        }
+        dft_small<8, false>(v[q]);
+        // natural-order index j + r N/8: the Green's function, then the
+        // inverse first stage (all twiddles 1) writing x[8 j + r]
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const float g = gf(j + r * NB, l);
+            v[q][r].x *= g;
+            v[q][r].y *= g;
+        }
+        dft_small<8, true>(v[q]);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) io.buf[(8 * j + r) * TX + l] = v[q][r];
     }
-    dft_small<8, false>(v);
-    // natural-order index j + r N/8: the Green's function, then the inverse
-    // first stage (all twiddles 1) writing x[8 j + r]
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const float g = gf(j + r * LT, l);
-        v[r].x *= g;
-        v[r].y *= g;
-    }
-    dft_small<8, true>(v);
-#pragma unroll
-    for (int r = 0; r < 8; ++r) io.buf[(8 * j + r) * TX + l] = v[r];
     __syncthreads();
 }
 
@@ -228,7 +241,9 @@ template <int N> struct ZRadix {
 #endif
 
 template <int N, int TXW = 0>
-__global__ void __launch_bounds__(ZTile<N, TXW>::THREADS, ZPASS_MIN_BLOCKS) k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
+__global__ void __launch_bounds__(ZTile<N, TXW>::THREADS,
+                                  ZTile<N, TXW>::THREADS >= 1024 ? 1 : ZTile<N, TXW>::LT < N / 8 ? 2 : ZPASS_MIN_BLOCKS)
+    k_zpass_green(float2 *__restrict__ spec, Mesh m, float gs,
                                                                    const float2 *__restrict__ twid) {
     extern __shared__ __align__(16) float2 zsh[];
     constexpr int TX = ZTile<N, TXW>::TX;
