@@ -210,6 +210,9 @@ template <typename T, int R> struct PM : PMBase {
             zpass = true;
             if (lacc) CONAN_TRY(plane_setup());
         }
+        // CONAN_GRAD_KERNEL: cell or zm picks the gradient-mesh kernel at
+        // creation (before any autotuning)
+        if (const char *gk = getenv("CONAN_GRAD_KERNEL")) grad_zm = !strcmp(gk, "zm");
         CONAN_TRY(alloc((char **)&work, wbytes));
         CONAN_TRY(fft.bind(work, st));
         if (zpass) CONAN_TRY(fft2.bind(work, st));

@@ -295,6 +295,24 @@ def test_plane_transforms_and_z_pass_give_the_3d_potential(gpu, conan, Nm, f):
     assert rel(phis["fp32"], phis["fp64"]) < 2e-5
 
 
+@pytest.mark.parametrize("Nm,f", [(64, 1), (32, 2), (128, 1)])
+def test_gradient_mesh_kernels_give_the_same_kick(gpu, conan, monkeypatch, Nm, f):
+    """The gradient-mesh kernels the autotuner chooses between (one thread
+    per cell, z-marching tiles) do the same arithmetic: the kicked momenta
+    agree bit for bit."""
+    L = 100.0
+    X, Pm = _particles(3, Nm, f, L, 2.0, 11)
+    out = {}
+    for kern in ("cell", "zm"):
+        monkeypatch.setenv("CONAN_GRAD_KERNEL", kern)
+        g = conan.Gravity(3, Nm, f, L, precision="fp32")
+        g.set_state(X, Pm, 0.4, 0.4)
+        g.kick(0.4, 0.01)
+        out[kern] = g.state()[1]
+        g.close()
+    assert np.array_equal(out["cell"], out["zm"])
+
+
 @pytest.mark.parametrize("Nm,f,columns,mode", [(256, 1, 16, "1"), (64, 8, 16, "1"), (128, 2, 16, "1"),
                                                (64, 8, 32, "1"), (128, 2, 32, "1"), (64, 8, 32, "2")])
 def test_cluster_plane_pass_matches_cufft_planes(gpu, conan, monkeypatch, Nm, f, columns, mode):
