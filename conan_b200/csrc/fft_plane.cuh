@@ -179,10 +179,15 @@ template <int N, int KC, bool INV> __device__ inline void y_fft(float2 *Y, const
 // transforms plane z. acc: the integer deposit (2^-23 units), kscale = 2^-23 x
 // particle mass; spec: the half spectra (z, ky, kx) of every plane; clear:
 // zero the accumulator behind the reads (instead of a memset after).
+// unit >= 0: the particle mass is 2^(23 - unit), so a kscale - 1 is exactly
+// (a - 2^unit) kscale and its rounding to float is that of the integer
+// a - 2^unit scaled by the power of two kscale: one 64-bit integer
+// subtraction and one conversion instead of two FP64 conversions (the same
+// bits as k_acc_mesh); unit < 0 takes the FP64 formula.
 template <int N, int KC>
 __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
     k_plane_fwd(unsigned long long *__restrict__ acc, float2 *__restrict__ spec, Mesh m, double kscale,
-                const float2 *__restrict__ twid, int clear) {
+                const float2 *__restrict__ twid, int clear, int unit) {
     typedef PlaneT<N, KC> P;
     constexpr int M = P::M, EPL = P::EPL;
     namespace cg = cooperative_groups;
@@ -222,9 +227,18 @@ __global__ void __launch_bounds__(512, PlaneT<N, KC>::MINB)
             for (int j = 0; j < EPL; ++j) a[j] = __ldcs(row + lane + 32 * j);
         }
         float2 v[EPL];
+        if (unit >= 0) {
+            const long long one = 1ll << unit;
+            const float fs = (float)kscale;  // a power of two: exact
 #pragma unroll
-        for (int j = 0; j < EPL; ++j)
-            v[j] = make_float2((float)((double)a[j].x * kscale - 1.0), (float)((double)a[j].y * kscale - 1.0));
+            for (int j = 0; j < EPL; ++j)
+                v[j] = make_float2(__ll2float_rn((long long)a[j].x - one) * fs,
+                                   __ll2float_rn((long long)a[j].y - one) * fs);
+        } else {
+#pragma unroll
+            for (int j = 0; j < EPL; ++j)
+                v[j] = make_float2((float)((double)a[j].x * kscale - 1.0), (float)((double)a[j].y * kscale - 1.0));
+        }
         if constexpr (PREFETCH) {
             if (i + P::WARPS < P::RY) {
 #pragma unroll

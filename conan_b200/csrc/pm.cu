@@ -736,6 +736,14 @@ template <typename T, int R> struct PM : PMBase {
         cfg.attrs = &at;
         cfg.numAttrs = 1;
     }
+    // 23 - log2(mass) when the particle mass is a power of two 2^e with
+    // 0 <= e <= 23 (the mesh factor f is a power of two), else -1
+    int plane_unit() const {
+        int e = 0;
+        const double fm = std::frexp(mass, &e);  // mass = fm 2^e, fm in [0.5, 1)
+        if (fm != 0.5 || e - 1 < 0 || e - 1 > 23) return -1;
+        return 23 - (e - 1);
+    }
     template <int N, int KC> int plane_run(double gs) {
         if constexpr (sizeof(T) == 4 && PlaneT<N, KC>::OK) {
             cudaLaunchConfig_t cfg = plane_cfg<N, KC>();
@@ -744,7 +752,7 @@ template <typename T, int R> struct PM : PMBase {
             float2 *sp = reinterpret_cast<float2 *>(spec);
             CONAN_TIMED(prof, "plane_r2c", st,
                         CONAN_CUDA(cudaLaunchKernelEx(&cfg, k_plane_fwd<N, KC>, lacc, sp, mf, 0x1p-23 * mass,
-                                                      (const float2 *)ztw, plane_clear ? 1 : 0)));
+                                                      (const float2 *)ztw, plane_clear ? 1 : 0, plane_unit())));
             if (!plane_clear)
                 CONAN_TIMED(prof, "deposit_clear", st,
                             CONAN_CUDA(cudaMemsetAsync(lacc, 0, mf.cells * sizeof(unsigned long long), st)));
