@@ -27,7 +27,7 @@
 namespace conan {
 
 // Lines per CTA and threads per CTA for an n-point z transform: n / 8
-// threads per line (n / 16 at 1024 points). (At n = 1024, 4 lines per CTA instead of 8 measured
+// threads per line (n / 16 from 256 points up). (At n = 1024, 4 lines per CTA instead of 8 measured
 // slower: 31.0 against 30.0 ms per step of the 1024^3-mesh run.)
 // TX = 0 takes the default width; the autotuner also tries half and twice
 // the default (ZTile<N, TX>::OK says whether a width fits one CTA).
@@ -38,9 +38,18 @@ namespace conan {
 #ifndef ZPASS_LT1024
 #define ZPASS_LT1024 64
 #endif
+// The same at 512 points: 64, 32 or 16 threads per line (0.385, 0.371 and
+// 0.384 ms per pass on the 512^3 mesh), and at 256 points 32 or 16 (0.050
+// and 0.047 ms on the 256^3 mesh).
+#ifndef ZPASS_LT512
+#define ZPASS_LT512 32
+#endif
+#ifndef ZPASS_LT256
+#define ZPASS_LT256 16
+#endif
 template <int N, int TX_ = 0> struct ZTile {
     static constexpr int TX = TX_ ? TX_ : (N >= 256 ? 8 : 2048 / N);
-    static constexpr int LT = N == 1024 ? ZPASS_LT1024 : N / 8;  // threads per line
+    static constexpr int LT = N == 1024 ? ZPASS_LT1024 : N == 512 ? ZPASS_LT512 : N == 256 ? ZPASS_LT256 : N / 8;  // threads per line
     static constexpr int THREADS = TX * LT;
     static constexpr size_t SMEM = (size_t)TX * N * sizeof(float2) + (size_t)N * sizeof(float2);
     static constexpr bool OK = THREADS <= 1024 && SMEM <= 200 * 1024;
